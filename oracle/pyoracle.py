@@ -1,0 +1,294 @@
+"""Python access to the two CPU checkers (test infrastructure only).
+
+* ``liboracle.so`` -- the plain-C restatement of XPIR's NFLLWE reply path
+  (``oracle/xpir_oracle.c``).
+* ``_ref/xpir_ref`` -- the XPIR reference sources compiled unchanged, driven through
+  the reference's own libpir API (``oracle/ref/xpir_ref.cpp``).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU arms import this
+module.  The product library (``xpir_b200``) never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+REF_BIN = HERE / "_ref" / "xpir_ref"
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_lib = None
+
+
+def build(reference_root: str | None = None) -> None:
+    """Compile liboracle.so, and the reference checker when its sources are present."""
+    env = dict(os.environ, CC="gcc", CXX="g++")
+    subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so"], check=True, env=env)
+    ref = reference_root or "/root/reference"
+    if Path(ref, "crypto", "NFLlib.cpp").exists():
+        subprocess.run(["make", "-s", "-j8", "-C", str(HERE), "ref", f"REF={ref}"], check=True, env=env)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        L = ctypes.CDLL(str(LIB_PATH))
+        L.xo_modulus.restype = ctypes.c_uint64
+        L.xo_modulus.argtypes = [ctypes.c_uint32]
+        L.xo_tables.argtypes = [ctypes.c_uint32, ctypes.c_uint32, _u64p]
+        L.xo_tables_words.restype = ctypes.c_uint64
+        L.xo_tables_words.argtypes = [ctypes.c_uint32, ctypes.c_uint32]
+        L.xo_bits_per_coeff.restype = ctypes.c_uint32
+        L.xo_bits_per_coeff.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64]
+        L.xo_polys_for_bits.restype = ctypes.c_uint64
+        L.xo_polys_for_bits.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32]
+        L.xo_bitsplit.argtypes = [_u8p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32,
+                                  ctypes.c_uint32, ctypes.c_uint32, _u64p]
+        L.xo_ntt_phi.argtypes = [_u64p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32]
+        L.xo_intt_phi.argtypes = [_u64p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32]
+        L.xo_aggregate.argtypes = [_u8p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32,
+                                   ctypes.c_uint64, _u8p]
+        L.xo_import.argtypes = [_u8p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32,
+                                ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _u64p]
+        L.xo_query_primes.argtypes = [_u64p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, _u64p]
+        L.xo_reply_level.argtypes = [_u64p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
+                                     _u64p, ctypes.c_uint32, ctypes.c_uint32, _u64p]
+        L.xo_reimport.argtypes = [_u64p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
+                                  ctypes.c_uint32, _u64p]
+        L.xo_reply.restype = ctypes.c_uint64
+        L.xo_reply.argtypes = [_u64p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32,
+                               ctypes.POINTER(ctypes.c_uint32), _u64p, ctypes.c_uint32, ctypes.c_uint32,
+                               ctypes.c_uint32, _u64p]
+        L.xo_reply_count.restype = ctypes.c_uint64
+        L.xo_reply_count.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                     ctypes.c_uint32, ctypes.c_uint32]
+        _lib = L
+    return _lib
+
+
+def _p64(a: np.ndarray):
+    assert a.dtype == np.uint64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_u64p)
+
+
+def _p8(a: np.ndarray):
+    assert a.dtype == np.uint8 and a.flags.c_contiguous
+    return a.ctypes.data_as(_u8p)
+
+
+# ----------------------------------------------------------------------------------
+# Restatement (liboracle.so)
+# ----------------------------------------------------------------------------------
+
+def modulus(i: int) -> int:
+    return int(lib().xo_modulus(i))
+
+
+def moduli(m: int) -> list[int]:
+    return [modulus(i) for i in range(m)]
+
+
+def tables(N: int, m: int) -> np.ndarray:
+    out = np.zeros(int(lib().xo_tables_words(N, m)), dtype=np.uint64)
+    assert lib().xo_tables(N, m, _p64(out)) == 0
+    return out
+
+
+def bits_per_coeff(N: int, m: int, n0: int, k: int = 80) -> int:
+    return int(lib().xo_bits_per_coeff(N, m, k, n0))
+
+
+def polys_for_bits(total_bits: int, b: int, N: int) -> int:
+    return int(lib().xo_polys_for_bits(total_bits, b, N))
+
+
+def bitsplit(bufs: np.ndarray, nbufs: int, stride: int, bits: int, b: int, N: int, m: int) -> np.ndarray:
+    P = polys_for_bits(nbufs * bits, b, N)
+    out = np.zeros(P * m * N, dtype=np.uint64)
+    bufs = np.ascontiguousarray(bufs, dtype=np.uint8)
+    assert lib().xo_bitsplit(_p8(bufs), nbufs, stride, bits, b, N, m, _p64(out)) == 0
+    return out
+
+
+def ntt_phi(polys: np.ndarray, N: int, m: int) -> np.ndarray:
+    x = np.ascontiguousarray(polys, dtype=np.uint64).copy()
+    assert lib().xo_ntt_phi(_p64(x), x.size // (m * N), N, m) == 0
+    return x
+
+
+def intt_phi(polys: np.ndarray, N: int, m: int) -> np.ndarray:
+    x = np.ascontiguousarray(polys, dtype=np.uint64).copy()
+    assert lib().xo_intt_phi(_p64(x), x.size // (m * N), N, m) == 0
+    return x
+
+
+def aggregate(elements: np.ndarray, nb: int, L: int, stride: int, alpha: int, s: int) -> np.ndarray:
+    out = np.zeros(alpha * L, dtype=np.uint8)
+    elements = np.ascontiguousarray(elements, dtype=np.uint8)
+    lib().xo_aggregate(_p8(elements), nb, L, stride, alpha, s, _p8(out))
+    return out
+
+
+def import_db(elements: np.ndarray, nb: int, L: int, alpha: int, b: int, N: int, m: int,
+              stride: int | None = None) -> np.ndarray:
+    stride = L if stride is None else stride
+    groups = -(-nb // alpha)
+    P = polys_for_bits(8 * alpha * L, b, N)
+    out = np.zeros(groups * P * m * N, dtype=np.uint64)
+    elements = np.ascontiguousarray(elements, dtype=np.uint8)
+    assert lib().xo_import(_p8(elements), nb, L, stride, alpha, b, N, m, _p64(out)) == 0
+    return out
+
+
+def query_primes(query: np.ndarray, N: int, m: int) -> np.ndarray:
+    q = np.ascontiguousarray(query, dtype=np.uint64)
+    out = np.zeros_like(q)
+    lib().xo_query_primes(_p64(q), q.size // (2 * m * N), N, m, _p64(out))
+    return out
+
+
+def reply_level(db: np.ndarray, n_real: int, P: int, n_groups: int, n_i: int, query: np.ndarray,
+                N: int, m: int) -> np.ndarray:
+    out = np.zeros(n_groups * P * 2 * m * N, dtype=np.uint64)
+    db = np.ascontiguousarray(db, dtype=np.uint64)
+    q = np.ascontiguousarray(query, dtype=np.uint64)
+    assert lib().xo_reply_level(_p64(db), n_real, P, n_groups, n_i, _p64(q), N, m, _p64(out)) == 0
+    return out
+
+
+def reimport(replies: np.ndarray, n_elts: int, P: int, b: int, N: int, m: int) -> np.ndarray:
+    P2 = polys_for_bits(P * 128 * m * N, b, N)
+    out = np.zeros(n_elts * P2 * m * N, dtype=np.uint64)
+    r = np.ascontiguousarray(replies, dtype=np.uint64)
+    assert lib().xo_reimport(_p64(r), n_elts, P, b, N, m, _p64(out)) == 0
+    return out
+
+
+def reply(db: np.ndarray, n_real: int, P: int, n: list[int], query: np.ndarray, b: int, N: int,
+          m: int) -> np.ndarray:
+    d = len(n)
+    Pl = P
+    for _ in range(d - 1):
+        Pl = polys_for_bits(Pl * 128 * m * N, b, N)
+    out = np.zeros(Pl * 2 * m * N, dtype=np.uint64)
+    narr = (ctypes.c_uint32 * d)(*n)
+    db = np.ascontiguousarray(db, dtype=np.uint64)
+    q = np.ascontiguousarray(query, dtype=np.uint64)
+    got = lib().xo_reply(_p64(db), n_real, P, d, narr, _p64(q), b, N, m, _p64(out))
+    assert got == Pl, (got, Pl)
+    return out
+
+
+def reply_count(L: int, alpha: int, d: int, b: int, N: int, m: int) -> int:
+    return int(lib().xo_reply_count(L, alpha, d, b, N, m))
+
+
+# ----------------------------------------------------------------------------------
+# The reference itself (_ref/xpir_ref)
+# ----------------------------------------------------------------------------------
+
+def ref_available() -> bool:
+    return REF_BIN.exists() and os.access(REF_BIN, os.X_OK)
+
+
+def _ref(cmd: str, args: dict, threads: int | None = None) -> dict:
+    argv = [str(REF_BIN), cmd]
+    for k, v in args.items():
+        if v is None or v is False:
+            continue
+        argv.append("--" + k)
+        if v is not True:
+            argv.append(str(v))
+    env = dict(os.environ)
+    if threads is not None:
+        env["OMP_NUM_THREADS"] = str(threads)
+    res = subprocess.run(argv, capture_output=True, text=True, env=env)
+    line = res.stdout.strip().splitlines()[-1] if res.stdout.strip() else "{}"
+    out = json.loads(line) if line.startswith("{") else {}
+    out["returncode"] = res.returncode
+    if res.returncode not in (0, 1):
+        raise RuntimeError(f"xpir_ref {cmd} failed ({res.returncode}): {res.stderr[-2000:]}")
+    return out
+
+
+def params_str(N: int, m: int, k: int = 80) -> str:
+    return f"LWE:{k}:{N}:{60 * m}"
+
+
+def ref_run(N: int, m: int, n: list[int], alpha: int, db: np.ndarray, nfiles: int, L: int, keyseed: int,
+            chosen: int, query: np.ndarray | None = None, want_imported: bool = False,
+            extract: bool = True, threads: int | None = None) -> dict:
+    """Full reference round trip.  Returns the JSON summary plus 'query', 'reply',
+    optionally 'imported' and 'plain' as arrays."""
+    with tempfile.TemporaryDirectory() as td:
+        t = Path(td)
+        np.ascontiguousarray(db, dtype=np.uint8).tofile(t / "db.bin")
+        args = {"params": params_str(N, m), "alpha": alpha, "d": len(n), "n": ",".join(map(str, n)),
+                "nfiles": nfiles, "eltbytes": L, "db": t / "db.bin", "keyseed": keyseed, "chosen": chosen,
+                "reply-out": t / "r.bin", "skip-extract": not extract}
+        if query is not None:
+            np.ascontiguousarray(query, dtype=np.uint64).tofile(t / "qin.bin")
+            args["query-in"] = t / "qin.bin"
+        else:
+            args["query-out"] = t / "q.bin"
+        if want_imported:
+            args["imported-out"] = t / "imp.bin"
+        if extract:
+            args["plain-out"] = t / "plain.bin"
+        out = _ref("run", args, threads)
+        out["reply"] = np.fromfile(t / "r.bin", dtype=np.uint64)
+        out["query"] = query if query is not None else np.fromfile(t / "q.bin", dtype=np.uint64)
+        if want_imported:
+            out["imported"] = np.fromfile(t / "imp.bin", dtype=np.uint64)
+        if extract and (t / "plain.bin").exists():
+            out["plain"] = np.fromfile(t / "plain.bin", dtype=np.uint8)
+        return out
+
+
+def ref_extract(N: int, m: int, n: list[int], alpha: int, L: int, keyseed: int, reply: np.ndarray) -> np.ndarray:
+    """Decrypt replies with the reference's PIRReplyExtraction and the seeded key."""
+    with tempfile.TemporaryDirectory() as td:
+        t = Path(td)
+        np.ascontiguousarray(reply, dtype=np.uint64).tofile(t / "r.bin")
+        _ref("extract", {"params": params_str(N, m), "alpha": alpha, "d": len(n), "n": ",".join(map(str, n)),
+                         "eltbytes": L, "keyseed": keyseed, "reply-in": t / "r.bin", "plain-out": t / "p.bin"})
+        return np.fromfile(t / "p.bin", dtype=np.uint8)
+
+
+def ref_info(N: int, m: int, n0: int) -> dict:
+    return _ref("info", {"params": params_str(N, m), "n": n0})
+
+
+def ref_tables(N: int, m: int) -> np.ndarray:
+    with tempfile.TemporaryDirectory() as td:
+        _ref("tables", {"params": params_str(N, m), "n": 1, "out": Path(td) / "t.bin"})
+        return np.fromfile(Path(td) / "t.bin", dtype=np.uint64)
+
+
+def ref_bitsplit(N: int, m: int, bufs: np.ndarray, nbufs: int, bits: int, b: int, stride: int,
+                 ntt: bool = False) -> np.ndarray:
+    with tempfile.TemporaryDirectory() as td:
+        t = Path(td)
+        np.ascontiguousarray(bufs, dtype=np.uint8).tofile(t / "in.bin")
+        _ref("deser" if ntt else "bitsplit",
+             {"params": params_str(N, m), "n": 1, "in": t / "in.bin", "nbufs": nbufs, "bufbits": bits,
+              "bufstride": stride, "bits": b, "out": t / "o.bin"})
+        return np.fromfile(t / "o.bin", dtype=np.uint64)
+
+
+def ref_ntt(N: int, m: int, polys: np.ndarray) -> np.ndarray:
+    with tempfile.TemporaryDirectory() as td:
+        t = Path(td)
+        np.ascontiguousarray(polys, dtype=np.uint64).tofile(t / "in.bin")
+        _ref("ntt", {"params": params_str(N, m), "n": 1, "in": t / "in.bin", "out": t / "o.bin"})
+        return np.fromfile(t / "o.bin", dtype=np.uint64)

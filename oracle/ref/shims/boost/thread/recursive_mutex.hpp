@@ -1,0 +1,2 @@
+// Stand-in: boost::recursive_mutex is provided by the boost/thread.hpp shim.
+#include <boost/thread.hpp>

@@ -1,0 +1,15 @@
+// Force-included (g++ -include) ahead of every reference source compiled as the parity
+// checker.  The reference was written against older toolchains whose standard headers
+// pulled these in transitively; g++ 13 does not.  Test infrastructure only.
+#ifndef XPIR_REF_PRELUDE_H
+#define XPIR_REF_PRELUDE_H
+#ifdef __cplusplus
+#include <cstdint>
+#include <cstring>
+#include <climits>
+#include <cmath>
+#include <string>
+#include <cassert>
+#endif
+#include <semaphore.h>  // SEM_VALUE_MAX, used by pir/shared_queue.hpp
+#endif

@@ -1,0 +1,487 @@
+/* xpir_oracle.c -- CPU restatement of XPIR's NFLLWE reply path (see xpir_oracle.h).
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the CUDA path, never part of the product.
+ * File:line references are to the XPIR reference sources (v0.2.0-beta).
+ */
+#include "xpir_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef unsigned __int128 u128;
+
+/* The 60-bit CRT moduli p_i = 2^61 - i*2^14 + 1, the primitive 2^14-th roots of unity
+ * and the inverses of 8192 modulo each p_i.  These must be the reference's exact values
+ * (crypto/NFLParams.cpp:30,36,40): every NTT-domain word depends on them. */
+static const uint64_t kModuli[XO_MAX_MODULI] = {
+    2305843009213317121ULL, 2305843009213120513ULL, 2305843009212694529ULL, 2305843009212399617ULL,
+    2305843009211662337ULL, 2305843009211596801ULL, 2305843009211400193ULL, 2305843009210580993ULL,
+    2305843009210515457ULL, 2305843009210023937ULL, 2305843009209057281ULL, 2305843009208795137ULL,
+    2305843009208713217ULL, 2305843009208123393ULL, 2305843009207468033ULL, 2305843009206976513ULL,
+    2305843009206845441ULL};
+static const uint64_t kRoots2p14[XO_MAX_MODULI] = {
+    1187132827279672845ULL, 753478288701480417ULL,  717492273700781398ULL,  1965831349000139179ULL,
+    2188074825493578002ULL, 232964966911499637ULL,  395215708149128273ULL,  241993652537061162ULL,
+    370764889455808762ULL,  1598724739621481826ULL, 610870591815427803ULL,  1880981984715338041ULL,
+    1389374064030612248ULL, 1508488901479281364ULL, 2111887543055470169ULL, 2020509703903079203ULL,
+    1120240637471598814ULL};
+static const uint64_t kInv8192[XO_MAX_MODULI] = {
+    2305561534236606511ULL, 2305561534236409927ULL, 2305561534235983995ULL, 2305561534235689119ULL,
+    2305561534234951929ULL, 2305561534234886401ULL, 2305561534234689817ULL, 2305561534233870717ULL,
+    2305561534233805189ULL, 2305561534233313729ULL, 2305561534232347191ULL, 2305561534232085079ULL,
+    2305561534232003169ULL, 2305561534231413417ULL, 2305561534230758137ULL, 2305561534230266677ULL,
+    2305561534230135621ULL};
+
+uint64_t xo_modulus(uint32_t i) { return i < XO_MAX_MODULI ? kModuli[i] : 0; }
+
+static uint32_t ilog2(uint64_t x) {
+  uint32_t r = 0;
+  while (x > 1) {
+    x >>= 1;
+    r++;
+  }
+  return r;
+}
+
+static int valid_shape(uint32_t N, uint32_t m) {
+  return m >= 1 && m <= XO_MAX_MODULI && N >= 4 && N <= 8192 && (N & (N - 1)) == 0;
+}
+
+/* Full modular product (crypto/NFLlib.hpp:272-275). */
+static inline uint64_t mulmod(uint64_t x, uint64_t y, uint64_t p) { return (uint64_t)(((u128)x * y) % p); }
+
+/* Shoup factor floor(y * 2^64 / p), truncated to 64 bits (crypto/NFLlib.hpp:580,
+ * pir/replyGenerator/PIRReplyGeneratorNFL_internal.cpp:764). */
+static inline uint64_t shoup(uint64_t y, uint64_t p) { return (uint64_t)(((u128)y << 64) / p); }
+
+/* x*y mod p from the Shoup factor, one final conditional subtraction
+ * (crypto/NFLlib.hpp:282-289). */
+static inline uint64_t mulmod_shoup(uint64_t x, uint64_t y, uint64_t ys, uint64_t p) {
+  uint64_t q = (uint64_t)(((u128)x * ys) >> 64);
+  uint64_t r = x * y - q * p;
+  return r >= p ? r - p : r;
+}
+
+/* Lazy multiply-accumulate: rop += x*y - q*p (mod 2^64), then at most one subtraction of
+ * p.  The accumulator is not canonical and its bits depend on the order of the calls
+ * (crypto/NFLlib.hpp:303-321). */
+static inline uint64_t mac_shoup(uint64_t rop, uint64_t x, uint64_t y, uint64_t ys, uint64_t p) {
+  uint64_t q = (uint64_t)(((u128)x * ys) >> 64);
+  rop += x * y - q * p;
+  return rop >= p ? rop - p : rop;
+}
+
+uint64_t xo_tables_words(uint32_t N, uint32_t m) { return (uint64_t)m * (1 + 8 * (uint64_t)N) + N; }
+
+/* Powers of w laid out layer by layer: N/2 powers of w, then N/4 of w^2, ... (the
+ * table walk of crypto/NFLlib.hpp:571-586). */
+static void layer_powers(uint64_t *tab, uint64_t *tabs, uint64_t w, uint32_t N, uint64_t p) {
+  for (uint32_t K = N; K >= 2; K >>= 1) {
+    uint64_t wi = 1;
+    for (uint32_t i = 0; i < K / 2; i++) {
+      *tab++ = wi;
+      *tabs++ = shoup(wi, p);
+      wi = mulmod(wi, w, p);
+    }
+    w = mulmod(w, w, p);
+  }
+  *tab = 0; /* the N-th slot is never written by the reference; keep it defined */
+  *tabs = 0;
+}
+
+/* crypto/NFLlib.cpp:44-194 (the GMP lifting integers are not needed on this path). */
+int xo_tables(uint32_t N, uint32_t m, uint64_t *out) {
+  if (!valid_shape(N, m)) return -1;
+  const uint32_t logN = ilog2(N);
+  uint64_t *o = out;
+  for (uint32_t c = 0; c < m; c++) {
+    const uint64_t p = kModuli[c];
+    uint64_t *phis = o + 1, *phis_s = phis + N, *w = phis_s + N, *w_s = w + N;
+    uint64_t *iphis = w_s + N, *iphis_s = iphis + N, *iw = iphis_s + N, *iw_s = iw + N;
+    o[0] = p;
+    /* phi: the 2^14-th root squared (13 - log2 N) times is a primitive 2N-th root. */
+    uint64_t phi = kRoots2p14[c];
+    for (int i = 0; i < 13 - (int)logN; i++) phi = mulmod(phi, phi, p);
+    uint64_t t = 1;
+    for (uint32_t i = 0; i < N; i++) {
+      phis[i] = t;
+      phis_s[i] = shoup(t, p);
+      t = mulmod(t, phi, p);
+    }
+    /* t = phi^N; phi^N * phi^(N-1) = phi^(2N-1) = phi^-1. */
+    const uint64_t invphi = mulmod(t, phis[N - 1], p);
+    const uint64_t invN = mulmod(kInv8192[c], 8192 / N, p);
+    t = invN;
+    for (uint32_t i = 0; i < N; i++) {
+      iphis[i] = t;
+      iphis_s[i] = shoup(t, p);
+      t = mulmod(t, invphi, p);
+    }
+    layer_powers(w, w_s, mulmod(phi, phi, p), N, p);
+    layer_powers(iw, iw_s, mulmod(invphi, invphi, p), N, p);
+    o += 1 + 8 * (uint64_t)N;
+  }
+  /* Bit reversal over log2 N bits; it is an involution, so it is its own inverse. */
+  for (uint32_t i = 0; i < N; i++) {
+    uint32_t r = 0, ii = i;
+    for (uint32_t h = 1; h < N; h <<= 1) {
+      r = (r << 1) | (ii & 1);
+      ii >>= 1;
+    }
+    o[i] = r;
+  }
+  return 0;
+}
+
+/* crypto/NFLLWE.cpp:656-668 with noiseUB = 5k/2 (integer) from crypto/NFLLWE.cpp:84. */
+uint32_t xo_bits_per_coeff(uint32_t N, uint32_t m, uint32_t k, uint64_t n0) {
+  double berr = (double)(uint64_t)(5 * (uint64_t)k / 2);
+  double nb_sum = (double)n0;
+  double p_size = (double)(60 * m);
+  double bits = floor(((p_size - 1) - log2(nb_sum) - log2(berr) - log2((double)N)) / 2.0);
+  return bits > 0 ? (uint32_t)bits : 0;
+}
+
+/* crypto/NFLlib.cpp:379 (double arithmetic, as the reference). */
+uint64_t xo_polys_for_bits(uint64_t total_bits, uint32_t b, uint32_t N) {
+  return (uint64_t)ceil((double)total_bits / (double)((uint64_t)b * N));
+}
+
+/* nbits (<= 64) bits of the concatenated stream from bit pos; zeros past its end. */
+static uint64_t stream_bits(const uint8_t *bufs, uint64_t nbufs, uint64_t stride, uint64_t bpb, uint64_t pos,
+                            uint32_t nbits) {
+  uint64_t v = 0;
+  uint32_t got = 0;
+  while (got < nbits) {
+    uint64_t bi = pos / bpb;
+    if (bi >= nbufs) break;
+    uint64_t off = pos - bi * bpb;
+    uint64_t avail = bpb - off;
+    uint32_t take = nbits - got;
+    if (take > avail) take = (uint32_t)avail;
+    const uint8_t *p = bufs + bi * stride + (off >> 3);
+    uint32_t sh = (uint32_t)(off & 7), nb = (sh + take + 7) / 8;
+    u128 w = 0;
+    for (uint32_t i = 0; i < nb; i++) w |= (u128)p[i] << (8 * i);
+    uint64_t val = (uint64_t)(w >> sh);
+    if (take < 64) val &= (1ULL << take) - 1;
+    v |= val << got;
+    got += take;
+    pos += take;
+  }
+  return v;
+}
+
+/* The reference's bit splitter walks the buffers with byte-unaligned 64-bit loads and
+ * carries partial sub-chunks across buffer boundaries (crypto/NFLlib.cpp:672-809); its
+ * output is that of a plain LSB-first bit stream over the concatenated buffers:
+ * coefficient k of poly j is bits [(jN+k)b, (jN+k+1)b), zero past the data.
+ * b <= 56: that value, copied to every modulus (crypto/NFLlib.cpp:812-839).
+ * b > 56: the value is cut into 56-bit sub-chunks s_t (the last one shorter) and
+ * modulus i receives sum_t mulmod(s_t, 2^(56t) mod p_i), each term reduced but the sum
+ * not (crypto/NFLlib.cpp:882-916). */
+int xo_bitsplit(const uint8_t *bufs, uint64_t nbufs, uint64_t buf_stride, uint64_t bits_per_buffer, uint32_t b,
+                uint32_t N, uint32_t m, uint64_t *out) {
+  if (!valid_shape(N, m) || b == 0 || b > 56 * 4) return -1;
+  const uint64_t total = nbufs * bits_per_buffer;
+  const uint64_t P = xo_polys_for_bits(total, b, N);
+  const uint32_t nsub = (b + 55) / 56;
+  uint64_t mult[XO_MAX_MODULI][4];
+  for (uint32_t c = 0; c < m; c++) {
+    mult[c][0] = 1;
+    for (uint32_t t = 1; t < nsub; t++) mult[c][t] = mulmod(mult[c][t - 1], 1ULL << 56, kModuli[c]);
+  }
+#pragma omp parallel for schedule(static)
+  for (int64_t j = 0; j < (int64_t)P; j++) {
+    for (uint32_t k = 0; k < N; k++) {
+      const uint64_t chunk = (uint64_t)j * N + k;
+      const uint64_t pos = chunk * b;
+      uint64_t *o = out + (uint64_t)j * m * N + k;
+      if (nsub == 1) {
+        uint64_t v = pos < total ? stream_bits(bufs, nbufs, buf_stride, bits_per_buffer, pos, b) : 0;
+        for (uint32_t c = 0; c < m; c++) o[(uint64_t)c * N] = v;
+      } else {
+        uint64_t sub[4] = {0, 0, 0, 0};
+        for (uint32_t t = 0; t < nsub; t++) {
+          uint32_t sz = (t + 1 < nsub) ? 56 : b - 56 * (nsub - 1);
+          uint64_t sp = pos + 56ULL * t;
+          sub[t] = sp < total ? stream_bits(bufs, nbufs, buf_stride, bits_per_buffer, sp, sz) : 0;
+        }
+        for (uint32_t c = 0; c < m; c++) {
+          uint64_t acc = 0;
+          for (uint32_t t = 0; t < nsub; t++) acc += mulmod(sub[t], mult[c][t], kModuli[c]);
+          o[(uint64_t)c * N] = acc;
+        }
+      }
+    }
+  }
+  return 0;
+}
+
+/* Harvey's lazy decimation-in-frequency NTT as modified by XPIR (crypto/NFLlib.hpp:450-537):
+ * log2(N)-2 radix-2 layers with inputs and outputs in [0, 2p), then the last two layers
+ * fused per group of four.  Natural order in, bit-reversed order out. */
+static void ntt_lazy(uint64_t *x, const uint64_t *w, const uint64_t *ws, uint32_t N, uint64_t p) {
+  const uint64_t p2 = 2 * p;
+  if (N == 2) {
+    uint64_t u0 = x[0], u1 = x[1];
+    uint64_t t0 = u0 + u1, t1 = u0 - u1;
+    t0 -= (t0 >= p2) ? p2 : 0;
+    t1 += ((int64_t)t1 < 0) ? p2 : 0;
+    x[0] = t0;
+    x[1] = t1;
+    return;
+  }
+  const uint32_t layers = ilog2(N) - 2;
+  for (uint32_t l = 0; l < layers; l++) {
+    const uint32_t len = N >> l, half = len >> 1;
+    for (uint32_t base = 0; base < N; base += len) {
+      for (uint32_t i = 0; i < half; i++) {
+        uint64_t u0 = x[base + i], u1 = x[base + i + half];
+        uint64_t t0 = u0 + u1;
+        t0 -= (t0 >= p2) ? p2 : 0;
+        uint64_t t1 = u0 - u1 + p2;
+        uint64_t q = (uint64_t)(((u128)t1 * ws[i]) >> 64);
+        x[base + i] = t0;
+        x[base + i + half] = t1 * w[i] - q * p;
+      }
+    }
+    w += half;
+    ws += half;
+  }
+  /* w now points at the 4-point layer: w[1] is the primitive 4th root. */
+  for (uint32_t base = 0; base < N; base += 4) {
+    uint64_t *y = x + base;
+    uint64_t u0 = y[0], u1 = y[1], u2 = y[2], u3 = y[3];
+    uint64_t v0 = u0 + u2;
+    v0 -= (v0 >= p2) ? p2 : 0;
+    uint64_t v2 = u0 - u2;
+    v2 += ((int64_t)v2 < 0) ? p2 : 0;
+    uint64_t v1 = u1 + u3;
+    v1 -= (v1 >= p2) ? p2 : 0;
+    uint64_t t = u1 - u3 + p2;
+    uint64_t q = (uint64_t)(((u128)t * ws[1]) >> 64);
+    uint64_t v3 = t * w[1] - q * p;
+    uint64_t z0 = v0 + v1;
+    z0 -= (z0 >= p2) ? p2 : 0;
+    uint64_t z1 = v0 - v1;
+    z1 += ((int64_t)z1 < 0) ? p2 : 0;
+    uint64_t z2 = v2 + v3;
+    z2 -= (z2 >= p2) ? p2 : 0;
+    uint64_t z3 = v2 - v3;
+    z3 += ((int64_t)z3 < 0) ? p2 : 0;
+    y[0] = z0;
+    y[1] = z1;
+    y[2] = z2;
+    y[3] = z3;
+  }
+}
+
+int xo_ntt_phi(uint64_t *polys, uint64_t npolys, uint32_t N, uint32_t m) {
+  if (!valid_shape(N, m)) return -1;
+  uint64_t *tab = (uint64_t *)malloc(xo_tables_words(N, m) * 8);
+  if (!tab) return -2;
+  xo_tables(N, m, tab);
+#pragma omp parallel for schedule(static)
+  for (int64_t j = 0; j < (int64_t)npolys; j++) {
+    for (uint32_t c = 0; c < m; c++) {
+      const uint64_t *t = tab + (uint64_t)c * (1 + 8 * (uint64_t)N);
+      const uint64_t p = t[0], *phis = t + 1, *phis_s = phis + N, *w = phis_s + N, *ws = w + N;
+      uint64_t *x = polys + ((uint64_t)j * m + c) * N;
+      for (uint32_t i = 0; i < N; i++) x[i] = mulmod_shoup(x[i], phis[i], phis_s[i], p);
+      ntt_lazy(x, w, ws, N, p);
+    }
+  }
+  free(tab);
+  return 0;
+}
+
+/* crypto/NFLlib.hpp:548-566 and 613-626: bit-reverse, forward lazy NTT with the inverse
+ * roots, bit-reverse back, then multiply by N^-1 phi^-i (fully reduced). */
+int xo_intt_phi(uint64_t *polys, uint64_t npolys, uint32_t N, uint32_t m) {
+  if (!valid_shape(N, m)) return -1;
+  uint64_t *tab = (uint64_t *)malloc(xo_tables_words(N, m) * 8);
+  if (!tab) return -2;
+  xo_tables(N, m, tab);
+  const uint64_t *rev = tab + (uint64_t)m * (1 + 8 * (uint64_t)N);
+#pragma omp parallel for schedule(static)
+  for (int64_t j = 0; j < (int64_t)npolys; j++) {
+    uint64_t *y = (uint64_t *)malloc((size_t)N * 8);
+    for (uint32_t c = 0; c < m; c++) {
+      const uint64_t *t = tab + (uint64_t)c * (1 + 8 * (uint64_t)N);
+      const uint64_t p = t[0], *iphis = t + 1 + 4 * (uint64_t)N, *iphis_s = iphis + N;
+      const uint64_t *iw = iphis_s + N, *iws = iw + N;
+      uint64_t *x = polys + ((uint64_t)j * m + c) * N;
+      for (uint32_t i = 0; i < N; i++) y[rev[i]] = x[i];
+      ntt_lazy(y, iw, iws, N, p);
+      for (uint32_t i = 0; i < N; i++) x[rev[i]] = y[i];
+      for (uint32_t i = 0; i < N; i++) x[i] = mulmod_shoup(x[i], iphis[i], iphis_s[i], p);
+    }
+    free(y);
+  }
+  free(tab);
+  return 0;
+}
+
+/* The reference fills one reused buffer per aggregated element s (importDataNFL calls
+ * readAggregatedStream for s = 0, 1, ... on the same calloc'd buffer,
+ * PIRReplyGeneratorNFL_internal.cpp:88,104-106).  For a group cut short by the end of the
+ * database (r < alpha real elements) the zero fill starts at slot r-1, not r, and stops
+ * at slot alpha-2 (DBHandler.cpp:21-24): slot r-1 (the last real element) reads as
+ * zeros and slot alpha-1 keeps what the previous group left there (element s*alpha-1,
+ * or zeros for s = 0). */
+void xo_aggregate(const uint8_t *elements, uint64_t nb_elements, uint64_t element_bytes, uint64_t element_stride,
+                  uint32_t alpha, uint64_t s, uint8_t *out) {
+  const uint64_t first = s * alpha;
+  const uint64_t end = (first + alpha - 1 < nb_elements - 1) ? first + alpha - 1 : nb_elements - 1;
+  const uint64_t padding = (first + alpha >= nb_elements) ? first + alpha - nb_elements : 0;
+  for (uint64_t i = first; i <= end; i++)
+    memcpy(out + (i % alpha) * element_bytes, elements + i * element_stride, element_bytes);
+  if (padding != 0) {
+    /* r = alpha - padding real elements sit in slots 0..r-1; the reference zeroes slots
+     * r-1 .. alpha-2 and never writes slot alpha-1 in this call, which therefore keeps
+     * the previous (full) group's last element, or the calloc zeros when s = 0. */
+    const uint64_t stale = alpha - 1;
+    if (s > 0)
+      memcpy(out + stale * element_bytes, elements + (first - 1) * element_stride, element_bytes);
+    else
+      memset(out + stale * element_bytes, 0, element_bytes);
+    memset(out + (end % alpha) * element_bytes, 0, element_bytes * padding);
+  }
+}
+
+int xo_import(const uint8_t *elements, uint64_t nb_elements, uint64_t element_bytes, uint64_t element_stride,
+              uint32_t alpha, uint32_t b, uint32_t N, uint32_t m, uint64_t *out) {
+  if (!valid_shape(N, m) || alpha == 0 || nb_elements == 0) return -1;
+  const uint64_t groups = (nb_elements + alpha - 1) / alpha;
+  const uint64_t bits = 8 * (uint64_t)alpha * element_bytes;
+  const uint64_t P = xo_polys_for_bits(bits, b, N);
+  uint8_t *agg = (uint8_t *)malloc(alpha * element_bytes + 16);
+  if (!agg) return -2;
+  for (uint64_t s = 0; s < groups; s++) {
+    xo_aggregate(elements, nb_elements, element_bytes, element_stride, alpha, s, agg);
+    int rc = xo_bitsplit(agg, 1, bits / 8 + 16, bits, b, N, m, out + s * P * m * N);
+    if (rc) {
+      free(agg);
+      return rc;
+    }
+  }
+  free(agg);
+  return xo_ntt_phi(out, groups * P, N, m);
+}
+
+void xo_query_primes(const uint64_t *y, uint64_t n, uint32_t N, uint32_t m, uint64_t *out) {
+  for (uint64_t i = 0; i < n; i++)
+    for (uint32_t h = 0; h < 2; h++)
+      for (uint32_t c = 0; c < m; c++)
+        for (uint32_t k = 0; k < N; k++) {
+          uint64_t idx = ((i * 2 + h) * m + c) * N + k;
+          out[idx] = shoup(y[idx], kModuli[c]);
+        }
+}
+
+int xo_reply_level(const uint64_t *db, uint64_t n_real, uint64_t P, uint64_t n_groups, uint64_t n_i,
+                   const uint64_t *query, uint32_t N, uint32_t m, uint64_t *out) {
+  if (!valid_shape(N, m)) return -1;
+  const uint64_t mN = (uint64_t)m * N, ct = 2 * mN;
+  uint64_t *primes = (uint64_t *)malloc(n_i * ct * 8);
+  if (!primes) return -2;
+  xo_query_primes(query, n_i, N, m, primes);
+  /* Chains are independent per (group, poly, half, modulus, coefficient); each one runs
+   * over the slots of its group strictly in order. */
+#pragma omp parallel for collapse(3) schedule(static)
+  for (int64_t j = 0; j < (int64_t)n_groups; j++) {
+    for (int64_t cp = 0; cp < (int64_t)P; cp++) {
+      for (int64_t c = 0; c < (int64_t)m; c++) {
+        const uint64_t p = kModuli[c];
+        uint64_t *ra = out + ((uint64_t)j * P + cp) * ct + c * N;
+        uint64_t *rb = ra + mN;
+        memset(ra, 0, N * 8);
+        memset(rb, 0, N * 8);
+        for (uint64_t q = 0; q < n_i; q++) {
+          const uint64_t e = (uint64_t)j * n_i + q;
+          const uint64_t *ya = query + q * ct + c * N, *yb = ya + mN;
+          const uint64_t *ysa = primes + q * ct + c * N, *ysb = ysa + mN;
+          if (e < n_real) {
+            const uint64_t *x = db + (e * P + cp) * mN + c * N;
+            for (uint32_t k = 0; k < N; k++) {
+              ra[k] = mac_shoup(ra[k], x[k], ya[k], ysa[k], p);
+              rb[k] = mac_shoup(rb[k], x[k], yb[k], ysb[k], p);
+            }
+          } else {
+            /* zero padding element (PIRReplyGeneratorNFL_internal.cpp:146-154): x = 0 */
+            for (uint32_t k = 0; k < N; k++) {
+              ra[k] = mac_shoup(ra[k], 0, ya[k], ysa[k], p);
+              rb[k] = mac_shoup(rb[k], 0, yb[k], ysb[k], p);
+            }
+          }
+        }
+      }
+    }
+  }
+  free(primes);
+  return 0;
+}
+
+int xo_reimport(const uint64_t *replies, uint64_t n_elts, uint64_t P, uint32_t b, uint32_t N, uint32_t m,
+                uint64_t *out) {
+  if (!valid_shape(N, m)) return -1;
+  const uint64_t ct_words = 2ULL * m * N, ct_bits = 64 * ct_words;
+  const uint64_t P2 = xo_polys_for_bits(P * ct_bits, b, N);
+  for (uint64_t e = 0; e < n_elts; e++) {
+    int rc = xo_bitsplit((const uint8_t *)(replies + e * P * ct_words), P, ct_words * 8, ct_bits, b, N, m,
+                         out + e * P2 * m * N);
+    if (rc) return rc;
+  }
+  return xo_ntt_phi(out, n_elts * P2, N, m);
+}
+
+uint64_t xo_reply(const uint64_t *db, uint64_t n_real, uint64_t P, uint32_t d, const uint32_t *n,
+                  const uint64_t *query, uint32_t b, uint32_t N, uint32_t m, uint64_t *out) {
+  if (!valid_shape(N, m) || d == 0) return 0;
+  const uint64_t mN = (uint64_t)m * N, ct_words = 2 * mN;
+  const uint64_t *in = db;
+  uint64_t *owned = NULL;
+  uint64_t in_real = n_real, in_P = P;
+  for (uint32_t lvl = 0; lvl < d; lvl++) {
+    uint64_t groups = 1;
+    for (uint32_t j = lvl + 1; j < d; j++) groups *= n[j];
+    uint64_t *rep = (uint64_t *)malloc(groups * in_P * ct_words * 8);
+    if (!rep) {
+      free(owned);
+      return 0;
+    }
+    xo_reply_level(in, in_real, in_P, groups, n[lvl], query, N, m, rep);
+    query += (uint64_t)n[lvl] * ct_words;
+    free(owned);
+    owned = NULL;
+    if (lvl + 1 == d) {
+      memcpy(out, rep, in_P * ct_words * 8);
+      free(rep);
+      return in_P;
+    }
+    const uint64_t P2 = xo_polys_for_bits(in_P * 64 * ct_words, b, N);
+    owned = (uint64_t *)malloc(groups * P2 * mN * 8);
+    if (!owned) {
+      free(rep);
+      return 0;
+    }
+    xo_reimport(rep, groups, in_P, b, N, m, owned);
+    free(rep);
+    in = owned;
+    in_real = groups;
+    in_P = P2;
+  }
+  return 0;
+}
+
+/* computeReplySizeInChunks: ceil over doubles per level, as the reference. */
+uint64_t xo_reply_count(uint64_t element_bytes, uint32_t alpha, uint32_t d, uint32_t b, uint32_t N, uint32_t m) {
+  const double abs_bits = (double)((uint64_t)b * N);
+  unsigned int out = (unsigned int)ceil((double)element_bytes * 8 * alpha / abs_bits);
+  const uint64_t ct_bytes = 2ULL * 64 * m * N / 8;
+  const uint64_t abs_bytes = (uint64_t)b * N / 8;
+  for (uint32_t i = 1; i < d; i++) out = (unsigned int)ceil(out * (double)ct_bytes / (double)abs_bytes);
+  return out;
+}
