@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 reply engine on XPIR's NFLLWE reply path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+
+A step is one reply generation for one query against a database already imported into
+HBM.  The default workload is the memory-bound single-query configuration: N=2048, two
+60-bit moduli ("LWE:80:2048:120"), d=1, alpha=1, 100,000 elements of 4 KB (imported:
+3.28 GB; one query: 100,000 ciphertexts = 6.55 GB).
+
+Reported (one JSON line on rank 0):
+  value      DB GB/s = imported-DB bytes streamed per step / reply time, with the query
+             resident in HBM; whole job = sum over ranks / max time over ranks.
+  e2e        the same metric through the C ABI with host buffers: the query copied from
+             pinned host memory and the reply copied back inside every timed step.
+  roofline   the reply kernel's algorithmic bytes (DB + query + reply) per launch over
+             its CUDA-event duration, against the measured HBM copy bandwidth.
+  cpu_baseline  the XPIR reference itself (oracle/_ref, compiled unchanged) on a bounded
+             sample of the same workload on this host's cores.
+Inputs are larger than L2 (9.8 GB per step vs 126 MB), so no L2 flush is needed.
+With --gpus N every rank runs an independent replica (its own database and query):
+the reply of one query has no cross-GPU exchange.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "reply-gen DB GB/s vs HBM peak; batched vs plain queries/s; p50/p99 latency"
+
+WORKLOADS = {
+    # name: N, m, n levels, alpha, elements, element bytes, chosen index, cpu-sample elements
+    "memory_bound": dict(N=2048, m=2, n=[100000], alpha=1, F=100000, L=4096, chosen=54321, sample=20000,
+                         desc="memory-bound single query: LWE:80:2048:120, d=1, alpha=1, 100000 x 4 KB"),
+    "plain": dict(N=1024, m=1, n=[1000], alpha=1, F=1000, L=12288, chosen=137, sample=1000,
+                  desc="plain single query: LWE:80:1024:60, d=1, alpha=1, 1000 x 12 KB"),
+    "recursive": dict(N=4096, m=3, n=[1024, 1024], alpha=16, F=1048576, L=256, chosen=5, sample=262144,
+                      desc="recursive: LWE:80:4096:180, d=2, 1024x1024 grid, alpha=16, 1048576 x 256 B"),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.tmp = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=self.tmp,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        self.tmp.flush()
+        rows = []
+        for line in Path(self.tmp.name).read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.tmp.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def synthetic_db(seed: int, F: int, L: int) -> np.ndarray:
+    return np.random.default_rng(seed).integers(0, 256, size=F * L, dtype=np.uint8)
+
+
+def synthetic_query(seed: int, n: list[int], N: int, m: int, moduli: list[int], out: np.ndarray) -> None:
+    """Uniform words reduced mod p per modulus, the shape and value range of a query
+    produced by XPIR's PIRQueryGenerator (crypto/NFLLWE.cpp:354-357)."""
+    rng = np.random.default_rng(seed)
+    q = out.reshape(sum(n), 2, m, N)
+    for c in range(m):
+        q[:, :, c, :] = rng.integers(0, moduli[c], size=(sum(n), 2, N), dtype=np.uint64)
+
+
+def run_reference(w: dict, steps: int, warmup: int, threads: int) -> dict:
+    """The XPIR reference (oracle/_ref) on a bounded sample of the workload."""
+    from oracle import pyoracle as po
+
+    if not po.ref_available():
+        return {"unavailable": "reference checker oracle/_ref/xpir_ref was not built"}
+    S = min(w["sample"], w["F"])
+    n = list(w["n"])
+    if len(n) == 1:
+        n = [-(-S // w["alpha"])]
+    db = synthetic_db(1, S, w["L"])
+    runs = []
+    for i in range(warmup + steps):
+        r = po.ref_run(w["N"], w["m"], n, w["alpha"], db, S, w["L"], keyseed=1000 + i, chosen=0, extract=False,
+                       threads=threads)
+        if i >= warmup:
+            runs.append(r)
+    imported = runs[0]["nb_elements"] * runs[0]["polys_per_element"] * w["m"] * w["N"] * 8
+    reply_s = [r["reply_s"] for r in runs]
+    import_s = [r["import_s"] for r in runs]
+    return {"value": imported / statistics.mean(reply_s) / 1e9, "reply_s": statistics.mean(reply_s),
+            "import_s": statistics.mean(import_s), "import_gbs": imported / statistics.mean(import_s) / 1e9,
+            "imported_bytes": imported, "elements": S, "n": n, "threads": runs[0]["omp_threads"],
+            "bits_per_coeff": runs[0]["bits_per_coeff"], "polys_per_element": runs[0]["polys_per_element"]}
+
+
+def reference_arm(args, w: dict, world: int, rank: int) -> int:
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    r = run_reference(w, args.steps, args.warmup, threads)
+    if "unavailable" in r:
+        print(json.dumps({"impl": "reference", "unavailable": r["unavailable"]}))
+        return 0
+    sample = (f"{r['elements']} elements of the workload (n={r['n']}, bits/coeff {r['bits_per_coeff']}), "
+              f"reply timed with omp_get_wtime boundaries as the reference prints them")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(r["value"], 4), "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(r["reply_s"] * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic: seeded uniform DB bytes; query from the reference's own PIRQueryGenerator",
+        "config": {"workload": w["desc"], "elements_sampled": r["elements"]},
+        "cpu_baseline": {"value": round(r["value"], 4), "unit": "GB/s", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": round(r["value"], 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "import": {"seconds": round(r["import_s"], 4), "gbs": round(r["import_gbs"], 4)},
+        "note": "the reference reply loop is OpenMP-parallel only over the polys of an element "
+                "(PIRReplyGeneratorNFL_internal.cpp:531-534); with 1 poly per element it runs on one thread",
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
+    import torch
+
+    import xpir_b200
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    device = local
+    torch.cuda.set_device(device)
+    N, m, n, alpha, F, L = w["N"], w["m"], w["n"], w["alpha"], w["F"], w["L"]
+    b = xpir_b200.bits_per_coeff(N, m, n[0])
+    ct_words = 2 * m * N
+    nq = sum(n)
+
+    log(f"[rank {rank}] generating {F * L / 1e9:.2f} GB database and {nq * ct_words * 8 / 1e9:.2f} GB query")
+    db = synthetic_db(1 + rank, F, L)
+    q_host = torch.empty(nq * ct_words, dtype=torch.int64, pin_memory=True)
+    moduli = xpir_b200.moduli(m)
+    synthetic_query(54321 + rank, n, N, m, moduli, q_host.numpy().view(np.uint64))
+
+    ctx = xpir_b200.Context(N, m, device=device)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=device)
+    # Import (not part of a step): timed separately, from host bytes.
+    t0 = time.perf_counter()
+    dbh = ctx.import_db(db, F, L, alpha, b)
+    import_s = time.perf_counter() - t0
+    del db
+    P = dbh.polys_per_element
+    Pl = P
+    for _ in range(len(n) - 1):
+        Pl = xpir_b200.polys_per_element(Pl * ct_words * 8, 1, b, N)
+    db_bytes = dbh.device_bytes
+    q_dev = q_host.to(f"cuda:{device}")
+    out_dev = torch.empty(Pl * ct_words, dtype=torch.int64, device=f"cuda:{device}")
+    out_host = torch.empty(Pl * ct_words, dtype=torch.int64, pin_memory=True)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---- value: query resident in HBM -------------------------------------------------
+    for _ in range(args.warmup):
+        ctx.reply(dbh, n, q_dev, out_dev)
+    torch.cuda.synchronize()
+    launches0 = ctx.launch_count
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(device) as clk:
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        t_start.record(stream)
+        for k in range(args.steps):
+            evs[k][0].record(stream)
+            ctx.reply(dbh, n, q_dev, out_dev)
+            evs[k][1].record(stream)
+        t_end.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    launches = ctx.launch_count - launches0
+    elapsed_ms = t_start.elapsed_time(t_end)
+    step_ms = [a.elapsed_time(b_) for a, b_ in evs]
+    clocks = clk.summary()
+
+    # ---- e2e: host query in, host reply out, through the C ABI -------------------------
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    ctx.reply(dbh, n, q_host, out_host)  # warm the host path once
+    barrier()
+    torch.cuda.synchronize()
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_end = torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    for _ in range(e2e_steps):
+        ctx.reply(dbh, n, q_host, out_host)
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = e_start.elapsed_time(e_end) / e2e_steps
+
+    # ---- aggregate over ranks ---------------------------------------------------------
+    if dist is not None:
+        t = torch.tensor([elapsed_ms, e2e_ms], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms, e2e_ms = t.tolist()
+    total_db = db_bytes * world
+    value = total_db * args.steps / (elapsed_ms / 1e3) / 1e9
+    e2e_value = total_db / (e2e_ms / 1e3) / 1e9
+
+    if rank == 0:
+        peaks = measured_peaks()
+        query_bytes = nq * ct_words * 8
+        reply_bytes = Pl * ct_words * 8
+        algo_bytes = db_bytes + query_bytes + reply_bytes if len(n) == 1 else None
+        kern_ms = statistics.mean(step_ms)
+        roofline = None
+        if algo_bytes:
+            achieved = algo_bytes / (kern_ms / 1e3) / 1e9
+            traffic = None
+            tf = ROOT / "profiles" / "reply_level_traffic.json"
+            if tf.exists():
+                t = json.loads(tf.read_text())
+                if t.get("workload") == args.workload:
+                    traffic = t.get("dram_bytes_per_launch")
+            roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                        "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
+                        "kernel": "reply_level_kernel", "peak_source": peaks["source"],
+                        "algorithmic_bytes_per_launch": algo_bytes, "kernel_ms": round(kern_ms, 4)}
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            r = run_reference(w, steps=1, warmup=0, threads=os.cpu_count() or 1)
+            if "unavailable" not in r:
+                cpu = {"value": round(r["value"], 4), "unit": "GB/s", "cores": r["threads"], "kind": "reference",
+                       "sample": f"{r['elements']} of {F} elements (n={r['n']}); reference reply time "
+                                 f"{r['reply_s']:.3f} s, import {r['import_s']:.3f} s",
+                       "import_gbs": round(r["import_gbs"], 4)}
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(elapsed_ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic: seeded uniform DB bytes; query words uniform mod p (PIRQueryGenerator shape)",
+            "config": {"workload": w["desc"], "N": N, "moduli": m, "d": len(n), "n": n, "alpha": alpha,
+                       "elements": F, "element_bytes": L, "bits_per_coeff": b, "polys_per_element": P,
+                       "imported_db_bytes": db_bytes, "query_bytes": query_bytes,
+                       "l2": "inputs larger than L2 (no flush needed)",
+                       "parallelism": f"replicas{world}" if world > 1 else "single GPU"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e_value, 3), "unit": "GB/s", "h2d_bytes_per_step": query_bytes,
+                    "d2h_bytes_per_step": reply_bytes, "ms_per_step": round(e2e_ms, 3)},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "import": {"seconds_wall": round(import_s, 4), "input_bytes": F * L, "imported_bytes": db_bytes},
+            "total_gbs": round((db_bytes + nq * ct_words * 8) * world * args.steps / (elapsed_ms / 1e3) / 1e9, 2),
+        }
+        print(json.dumps(line), flush=True)
+    dbh.free()
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--workload", default="memory_bound", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--elements", type=int, default=0,
+                    help="override the element count of a d=1 workload (profiling runs on a smaller case)")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    w = dict(WORKLOADS[args.workload])
+    if args.elements:
+        if len(w["n"]) != 1:
+            ap.error("--elements applies to d=1 workloads")
+        w.update(F=args.elements, n=[args.elements], sample=min(w["sample"], args.elements),
+                 desc=w["desc"].replace(f"{WORKLOADS[args.workload]['F']} x", f"{args.elements} x"))
+    if args.impl == "reference":
+        return reference_arm(args, w, world, rank)
+    return ours_arm(args, w, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

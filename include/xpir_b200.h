@@ -1,0 +1,124 @@
+/* xpir_b200.h -- C ABI of the B200 (sm_100a) reply engine for XPIR's NFLLWE path.
+ *
+ * The drop-in boundary: XPIR's PIRReplyGeneratorNFL_internal (the engine behind libpir's
+ * PIRReplyGenerator, GenericPIRReplyGenerator and PIRReplyGeneratorFactory("LWE")) is
+ * replaced by calls to these functions.  Plain pointers and sizes only; every function
+ * returns an XPIR_B200_* status (0 = success) and never aborts the process.
+ *
+ * Data formats are XPIR's, unchanged (little-endian u64 words):
+ *   query ciphertext  [a: m polys x N][b: m polys x N]   getCiphertextBitsize()/8 bytes
+ *                     (crypto/NFLLWEPublicParameters.cpp:82-86,148-151)
+ *   reply ciphertext  same layout, lazily reduced words, bit-identical to XPIR's
+ *   a query           the sum(n[i]) ciphertexts in push order (level 0 slots first),
+ *                     back to back, as PIRReplyGeneratorNFL_internal::pushQuery receives
+ *                     them (pir/replyGenerator/PIRReplyGeneratorNFL_internal.cpp:722-781)
+ *   database          nb_elements elements of element_bytes bytes, element i at
+ *                     elements + i*element_stride (the bytes DBHandler::readStream yields)
+ */
+#ifndef XPIR_B200_H
+#define XPIR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define XPIR_B200_API __attribute__((visibility("default")))
+#else
+#define XPIR_B200_API
+#endif
+
+#define XPIR_B200_OK 0
+#define XPIR_B200_ERR_ARG (-1)     /* invalid argument or unsupported shape */
+#define XPIR_B200_ERR_NOMEM (-2)   /* device or pinned-host allocation failed */
+#define XPIR_B200_ERR_CUDA (-3)    /* CUDA runtime error (see xpir_b200_last_cuda_error) */
+#define XPIR_B200_ERR_NODEV (-4)   /* no usable CUDA device */
+#define XPIR_B200_ERR_STATE (-5)   /* call out of order (e.g. incomplete query) */
+#define XPIR_B200_MAX_LEVELS 10    /* MAX_REC_LVL, pir/PIRParameters.hpp:22 */
+
+typedef struct xpir_b200_ctx xpir_b200_ctx; /* one (N, moduli) parameter set on one GPU */
+typedef struct xpir_b200_db xpir_b200_db;   /* an imported database resident in HBM */
+
+/* ---- library ------------------------------------------------------------------ */
+XPIR_B200_API const char *xpir_b200_version(void);
+XPIR_B200_API const char *xpir_b200_strerror(int status);
+/* Name of the last CUDA error seen by any call (diagnostics). */
+XPIR_B200_API const char *xpir_b200_last_cuda_error(void);
+XPIR_B200_API int xpir_b200_device_count(int *count);
+
+/* ---- sizing (host only; no GPU needed) ---------------------------------------- */
+/* Bits absorbed per coefficient for a query whose first dimension is n0:
+ * replaces NFLLWE::setandgetAbsBitPerCiphertext (crypto/NFLLWE.cpp:656-668). */
+XPIR_B200_API int32_t xpir_b200_bits_per_coeff(uint32_t poly_degree, uint32_t nb_moduli, uint32_t security_bits, uint64_t n0);
+/* Polynomials per (aggregated) element: NFLlib::deserializeDataNFL's polyNumber
+ * (crypto/NFLlib.cpp:379). */
+XPIR_B200_API uint64_t xpir_b200_polys_per_element(uint64_t element_bytes, uint32_t alpha, uint32_t bits_per_coeff,
+                                     uint32_t poly_degree);
+/* Number of reply ciphertexts: PIRReplyGeneratorNFL_internal::computeReplySizeInChunks
+ * (pir/replyGenerator/PIRReplyGeneratorNFL_internal.cpp:667-679). */
+XPIR_B200_API uint64_t xpir_b200_reply_count(uint64_t element_bytes, uint32_t alpha, uint32_t d, uint32_t bits_per_coeff,
+                               uint32_t poly_degree, uint32_t nb_moduli);
+/* The i-th 60-bit CRT modulus, 2^61 - i*2^14 + 1 (NFLlib::getmoduli, crypto/NFLParams.cpp:30);
+ * 0 when i is out of range. */
+XPIR_B200_API uint64_t xpir_b200_modulus(uint32_t i);
+/* Bytes of one query/reply ciphertext: NFLLWEPublicParameters::getCiphertextBitsize()/8
+ * (crypto/NFLLWEPublicParameters.cpp:148-151). */
+XPIR_B200_API uint64_t xpir_b200_ciphertext_bytes(uint32_t poly_degree, uint32_t nb_moduli);
+
+/* ---- context -------------------------------------------------------------------- */
+/* Parameter set "LWE:k:N:60*nb_moduli" on `device`: builds and uploads the NTT tables,
+ * the role of NFLlib::setNewParameters/configureNTT (crypto/NFLlib.cpp:44-228).  The
+ * context owns one CUDA stream; all its work is ordered on it. */
+XPIR_B200_API int xpir_b200_ctx_create(xpir_b200_ctx **ctx, int device, uint32_t poly_degree, uint32_t nb_moduli);
+XPIR_B200_API int xpir_b200_ctx_destroy(xpir_b200_ctx *ctx);
+/* The context's cudaStream_t, as a void pointer (for event timing by the caller). */
+XPIR_B200_API int xpir_b200_ctx_stream(xpir_b200_ctx *ctx, void **stream);
+/* Blocks until all work queued on the context has finished. */
+XPIR_B200_API int xpir_b200_ctx_synchronize(xpir_b200_ctx *ctx);
+/* Number of engine kernels launched on this context so far. */
+XPIR_B200_API int xpir_b200_ctx_launch_count(xpir_b200_ctx *ctx, uint64_t *count);
+
+/* ---- database import -------------------------------------------------------------- */
+/* Imports a database for queries whose aggregation is `alpha` and whose first dimension
+ * gives `bits_per_coeff`: aggregation as DBHandler::readAggregatedStream, bit split,
+ * CRT and NTT as NFLlib::deserializeDataNFL, for every aggregated element.  Replaces
+ * PIRReplyGeneratorNFL_internal::importDataNFL (…NFL_internal.cpp:79-158) behind
+ * libpir's PIRReplyGenerator::importData (pir/libpir.cpp:90-103).  `elements` is host
+ * memory when src_on_device == 0, device memory otherwise.  The zero padding of the
+ * index grid (…NFL_internal.cpp:146-154) is not materialised. */
+XPIR_B200_API int xpir_b200_db_import(xpir_b200_ctx *ctx, const void *elements, uint64_t nb_elements, uint64_t element_bytes,
+                        uint64_t element_stride, uint32_t alpha, uint32_t bits_per_coeff, int src_on_device,
+                        xpir_b200_db **db);
+/* Frees the device copy: the role of imported_database::~imported_database
+ * (pir/libpir.cpp:5-11). */
+XPIR_B200_API int xpir_b200_db_free(xpir_b200_db *db);
+/* Aggregated elements, polys per element, bits per coefficient and HBM bytes held. */
+XPIR_B200_API int xpir_b200_db_info(const xpir_b200_db *db, uint64_t *nb_aggregated, uint64_t *polys_per_element,
+                      uint32_t *bits_per_coeff, uint64_t *device_bytes);
+/* Copies the imported polys to host memory, in the reference's per-element layout
+ * [element][poly][modulus][coefficient] (nb_aggregated * P * m * N words). */
+XPIR_B200_API int xpir_b200_db_export(const xpir_b200_db *db, uint64_t *host_out, uint64_t capacity_words);
+
+/* ---- reply ---------------------------------------------------------------------- */
+/* Generates the reply of one query against an imported database: the level loop of
+ * PIRReplyGeneratorNFL_internal::generateReply (…NFL_internal.cpp:340-445) with the
+ * per-slot Shoup multiply-accumulate (crypto/NFLLWE.cpp:176-205) and the on-device
+ * re-import of each level's replies as the next level's database (…NFL_internal.cpp:
+ * 599-626).  `d` and `n` are PIRParameters.d and .n (pir/PIRParameters.hpp:24-29);
+ * prod(n) must be at least the number of aggregated elements.  `query` holds sum(n)
+ * ciphertexts (host memory if query_on_device == 0).  `replies` receives the final
+ * ciphertexts (host memory if out_on_device == 0), `capacity_bytes` long; their count
+ * is written to *nb_replies.  Replaces libpir's PIRReplyGenerator::generateReply
+ * (pir/libpir.cpp:106-135); the outputs are what popReply hands out. */
+XPIR_B200_API int xpir_b200_reply(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, const uint32_t *n, const void *query,
+                    int query_on_device, void *replies, uint64_t capacity_bytes, int out_on_device,
+                    uint64_t *nb_replies);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XPIR_B200_H */

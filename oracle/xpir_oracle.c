@@ -354,20 +354,26 @@ void xo_aggregate(const uint8_t *elements, uint64_t nb_elements, uint64_t elemen
 int xo_import(const uint8_t *elements, uint64_t nb_elements, uint64_t element_bytes, uint64_t element_stride,
               uint32_t alpha, uint32_t b, uint32_t N, uint32_t m, uint64_t *out) {
   if (!valid_shape(N, m) || alpha == 0 || nb_elements == 0) return -1;
+  if (b == 0 || b > 56 * 4) return -1;
   const uint64_t groups = (nb_elements + alpha - 1) / alpha;
   const uint64_t bits = 8 * (uint64_t)alpha * element_bytes;
   const uint64_t P = xo_polys_for_bits(bits, b, N);
-  uint8_t *agg = (uint8_t *)malloc(alpha * element_bytes + 16);
-  if (!agg) return -2;
-  for (uint64_t s = 0; s < groups; s++) {
-    xo_aggregate(elements, nb_elements, element_bytes, element_stride, alpha, s, agg);
-    int rc = xo_bitsplit(agg, 1, bits / 8 + 16, bits, b, N, m, out + s * P * m * N);
-    if (rc) {
-      free(agg);
-      return rc;
+  int failed = 0;
+  /* Aggregated elements are independent (xo_aggregate reproduces the reused buffer's
+   * state from the element indexes alone), so they are split in parallel. */
+#pragma omp parallel reduction(| : failed)
+  {
+    uint8_t *agg = (uint8_t *)malloc(alpha * element_bytes + 16);
+    if (!agg) failed = 1;
+#pragma omp for schedule(dynamic, 16)
+    for (int64_t s = 0; s < (int64_t)groups; s++) {
+      if (!agg) continue;
+      xo_aggregate(elements, nb_elements, element_bytes, element_stride, alpha, (uint64_t)s, agg);
+      if (xo_bitsplit(agg, 1, bits / 8 + 16, bits, b, N, m, out + (uint64_t)s * P * m * N)) failed = 1;
     }
+    free(agg);
   }
-  free(agg);
+  if (failed) return -2;
   return xo_ntt_phi(out, groups * P, N, m);
 }
 
@@ -385,42 +391,38 @@ int xo_reply_level(const uint64_t *db, uint64_t n_real, uint64_t P, uint64_t n_g
                    const uint64_t *query, uint32_t N, uint32_t m, uint64_t *out) {
   if (!valid_shape(N, m)) return -1;
   const uint64_t mN = (uint64_t)m * N, ct = 2 * mN;
-  uint64_t *primes = (uint64_t *)malloc(n_i * ct * 8);
-  if (!primes) return -2;
-  xo_query_primes(query, n_i, N, m, primes);
+  const uint32_t KB = 64; /* coefficients per work item */
+  const uint32_t nkb = N / KB;
   /* Chains are independent per (group, poly, half, modulus, coefficient); each one runs
-   * over the slots of its group strictly in order. */
-#pragma omp parallel for collapse(3) schedule(static)
+   * over the slots of its group strictly in order.  The query Shoup factors
+   * (pushQuery, PIRReplyGeneratorNFL_internal.cpp:756-767) are recomputed per use. */
+#pragma omp parallel for collapse(4) schedule(dynamic, 1)
   for (int64_t j = 0; j < (int64_t)n_groups; j++) {
     for (int64_t cp = 0; cp < (int64_t)P; cp++) {
       for (int64_t c = 0; c < (int64_t)m; c++) {
-        const uint64_t p = kModuli[c];
-        uint64_t *ra = out + ((uint64_t)j * P + cp) * ct + c * N;
-        uint64_t *rb = ra + mN;
-        memset(ra, 0, N * 8);
-        memset(rb, 0, N * 8);
-        for (uint64_t q = 0; q < n_i; q++) {
-          const uint64_t e = (uint64_t)j * n_i + q;
-          const uint64_t *ya = query + q * ct + c * N, *yb = ya + mN;
-          const uint64_t *ysa = primes + q * ct + c * N, *ysb = ysa + mN;
-          if (e < n_real) {
-            const uint64_t *x = db + (e * P + cp) * mN + c * N;
-            for (uint32_t k = 0; k < N; k++) {
-              ra[k] = mac_shoup(ra[k], x[k], ya[k], ysa[k], p);
-              rb[k] = mac_shoup(rb[k], x[k], yb[k], ysb[k], p);
-            }
-          } else {
-            /* zero padding element (PIRReplyGeneratorNFL_internal.cpp:146-154): x = 0 */
-            for (uint32_t k = 0; k < N; k++) {
-              ra[k] = mac_shoup(ra[k], 0, ya[k], ysa[k], p);
-              rb[k] = mac_shoup(rb[k], 0, yb[k], ysb[k], p);
+        for (int64_t kb = 0; kb < (int64_t)nkb; kb++) {
+          const uint64_t p = kModuli[c];
+          const uint64_t k0 = (uint64_t)kb * KB;
+          uint64_t *ra = out + ((uint64_t)j * P + cp) * ct + c * N + k0;
+          uint64_t *rb = ra + mN;
+          memset(ra, 0, KB * 8);
+          memset(rb, 0, KB * 8);
+          for (uint64_t q = 0; q < n_i; q++) {
+            const uint64_t e = (uint64_t)j * n_i + q;
+            const uint64_t *ya = query + q * ct + c * N + k0, *yb = ya + mN;
+            /* a slot past the real elements is an all-zero element
+             * (PIRReplyGeneratorNFL_internal.cpp:146-154) */
+            const uint64_t *x = e < n_real ? db + (e * P + cp) * mN + c * N + k0 : NULL;
+            for (uint32_t k = 0; k < KB; k++) {
+              const uint64_t xk = x ? x[k] : 0;
+              ra[k] = mac_shoup(ra[k], xk, ya[k], shoup(ya[k], p), p);
+              rb[k] = mac_shoup(rb[k], xk, yb[k], shoup(yb[k], p), p);
             }
           }
         }
       }
     }
   }
-  free(primes);
   return 0;
 }
 
@@ -429,11 +431,14 @@ int xo_reimport(const uint64_t *replies, uint64_t n_elts, uint64_t P, uint32_t b
   if (!valid_shape(N, m)) return -1;
   const uint64_t ct_words = 2ULL * m * N, ct_bits = 64 * ct_words;
   const uint64_t P2 = xo_polys_for_bits(P * ct_bits, b, N);
-  for (uint64_t e = 0; e < n_elts; e++) {
-    int rc = xo_bitsplit((const uint8_t *)(replies + e * P * ct_words), P, ct_words * 8, ct_bits, b, N, m,
-                         out + e * P2 * m * N);
-    if (rc) return rc;
+  int failed = 0;
+#pragma omp parallel for schedule(dynamic, 4) reduction(| : failed)
+  for (int64_t e = 0; e < (int64_t)n_elts; e++) {
+    if (xo_bitsplit((const uint8_t *)(replies + (uint64_t)e * P * ct_words), P, ct_words * 8, ct_bits, b, N, m,
+                    out + (uint64_t)e * P2 * m * N))
+      failed = 1;
   }
+  if (failed) return -1;
   return xo_ntt_phi(out, n_elts * P2, N, m);
 }
 

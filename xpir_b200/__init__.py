@@ -1,0 +1,234 @@
+"""Python binding of the B200 reply engine's C ABI (include/xpir_b200.h).
+
+This is plumbing for tests and benchmarks: every computation happens in the CUDA
+library ``libxpir_b200.so`` built in-tree by ``xpir_b200.build``.  There is no CPU
+compute path; if the library is missing or no GPU is usable, calls raise.
+
+The class names follow XPIR's vocabulary: a :class:`Context` is one NFLLWE parameter
+set ("LWE:k:N:60m") on one GPU, a :class:`Database` is an imported database resident in
+HBM (XPIR's ``imported_database``), and :meth:`Context.reply` is
+``PIRReplyGenerator::generateReply`` for one query.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libxpir_b200.so"
+
+OK = 0
+ERR_ARG = -1
+ERR_NOMEM = -2
+ERR_CUDA = -3
+ERR_NODEV = -4
+ERR_STATE = -5
+
+_lib = None
+
+
+class XpirError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        msg = _load().xpir_b200_strerror(status).decode()
+        cuda = _load().xpir_b200_last_cuda_error().decode()
+        super().__init__(f"{where}: {msg} (status {status}, last CUDA error {cuda})")
+        self.status = status
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m xpir_b200.build` "
+                               "(the engine has no CPU fallback)")
+        L = ctypes.CDLL(str(LIB_PATH))
+        c_u32, c_u64, c_i32, vp = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_void_p
+        L.xpir_b200_version.restype = ctypes.c_char_p
+        L.xpir_b200_strerror.restype = ctypes.c_char_p
+        L.xpir_b200_strerror.argtypes = [ctypes.c_int]
+        L.xpir_b200_last_cuda_error.restype = ctypes.c_char_p
+        L.xpir_b200_device_count.argtypes = [ctypes.POINTER(ctypes.c_int)]
+        L.xpir_b200_bits_per_coeff.restype = c_i32
+        L.xpir_b200_bits_per_coeff.argtypes = [c_u32, c_u32, c_u32, c_u64]
+        L.xpir_b200_polys_per_element.restype = c_u64
+        L.xpir_b200_polys_per_element.argtypes = [c_u64, c_u32, c_u32, c_u32]
+        L.xpir_b200_reply_count.restype = c_u64
+        L.xpir_b200_reply_count.argtypes = [c_u64, c_u32, c_u32, c_u32, c_u32, c_u32]
+        L.xpir_b200_ciphertext_bytes.restype = c_u64
+        L.xpir_b200_ciphertext_bytes.argtypes = [c_u32, c_u32]
+        L.xpir_b200_modulus.restype = c_u64
+        L.xpir_b200_modulus.argtypes = [c_u32]
+        L.xpir_b200_ctx_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, c_u32, c_u32]
+        L.xpir_b200_ctx_destroy.argtypes = [vp]
+        L.xpir_b200_ctx_stream.argtypes = [vp, ctypes.POINTER(vp)]
+        L.xpir_b200_ctx_synchronize.argtypes = [vp]
+        L.xpir_b200_ctx_launch_count.argtypes = [vp, ctypes.POINTER(c_u64)]
+        L.xpir_b200_db_import.argtypes = [vp, vp, c_u64, c_u64, c_u64, c_u32, c_u32, ctypes.c_int,
+                                          ctypes.POINTER(vp)]
+        L.xpir_b200_db_free.argtypes = [vp]
+        L.xpir_b200_db_info.argtypes = [vp, ctypes.POINTER(c_u64), ctypes.POINTER(c_u64),
+                                        ctypes.POINTER(c_u32), ctypes.POINTER(c_u64)]
+        L.xpir_b200_db_export.argtypes = [vp, vp, c_u64]
+        L.xpir_b200_reply.argtypes = [vp, vp, c_u32, ctypes.POINTER(c_u32), vp, ctypes.c_int, vp, c_u64,
+                                      ctypes.c_int, ctypes.POINTER(c_u64)]
+        _lib = L
+    return _lib
+
+
+def lib():
+    return _load()
+
+
+def _check(status: int, where: str) -> None:
+    if status != OK:
+        raise XpirError(status, where)
+
+
+def version() -> str:
+    return _load().xpir_b200_version().decode()
+
+
+def device_count() -> int:
+    n = ctypes.c_int(0)
+    _load().xpir_b200_device_count(ctypes.byref(n))
+    return n.value
+
+
+def bits_per_coeff(N: int, m: int, n0: int, security_bits: int = 80) -> int:
+    return int(_load().xpir_b200_bits_per_coeff(N, m, security_bits, n0))
+
+
+def polys_per_element(element_bytes: int, alpha: int, b: int, N: int) -> int:
+    return int(_load().xpir_b200_polys_per_element(element_bytes, alpha, b, N))
+
+
+def reply_count(element_bytes: int, alpha: int, d: int, b: int, N: int, m: int) -> int:
+    return int(_load().xpir_b200_reply_count(element_bytes, alpha, d, b, N, m))
+
+
+def ciphertext_bytes(N: int, m: int) -> int:
+    return int(_load().xpir_b200_ciphertext_bytes(N, m))
+
+
+def modulus(i: int) -> int:
+    return int(_load().xpir_b200_modulus(i))
+
+
+def moduli(m: int) -> list[int]:
+    return [modulus(i) for i in range(m)]
+
+
+def _ptr(x) -> int:
+    """Address of a numpy array (host) or of anything exposing data_ptr() (device)."""
+    if isinstance(x, np.ndarray):
+        assert x.flags.c_contiguous
+        return x.ctypes.data
+    if hasattr(x, "data_ptr"):
+        return int(x.data_ptr())
+    return int(x)
+
+
+def _on_device(x) -> int:
+    return 0 if isinstance(x, np.ndarray) else int(getattr(x, "is_cuda", True))
+
+
+class Database:
+    """An imported database resident in HBM (XPIR's imported_database)."""
+
+    def __init__(self, ctx: "Context", handle: int):
+        self.ctx = ctx
+        self.handle = ctypes.c_void_p(handle)
+        n = ctypes.c_uint64()
+        P = ctypes.c_uint64()
+        b = ctypes.c_uint32()
+        nbytes = ctypes.c_uint64()
+        _check(_load().xpir_b200_db_info(self.handle, ctypes.byref(n), ctypes.byref(P), ctypes.byref(b),
+                                         ctypes.byref(nbytes)), "db_info")
+        self.nb_aggregated, self.polys_per_element = n.value, P.value
+        self.bits_per_coeff, self.device_bytes = b.value, nbytes.value
+
+    def export(self) -> np.ndarray:
+        words = self.nb_aggregated * self.polys_per_element * self.ctx.m * self.ctx.N
+        out = np.empty(words, dtype=np.uint64)
+        _check(_load().xpir_b200_db_export(self.handle, out.ctypes.data, words), "db_export")
+        return out
+
+    def free(self) -> None:
+        if self.handle:
+            _check(_load().xpir_b200_db_free(self.handle), "db_free")
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Context:
+    """One NFLLWE parameter set (poly degree N, m 60-bit moduli) on one GPU."""
+
+    def __init__(self, N: int, m: int, device: int = 0):
+        self.N, self.m, self.device = N, m, device
+        h = ctypes.c_void_p()
+        _check(_load().xpir_b200_ctx_create(ctypes.byref(h), device, N, m), "ctx_create")
+        self.handle = h
+        self.ct_words = 2 * m * N
+
+    @property
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        _check(_load().xpir_b200_ctx_stream(self.handle, ctypes.byref(s)), "ctx_stream")
+        return s.value or 0
+
+    def synchronize(self) -> None:
+        _check(_load().xpir_b200_ctx_synchronize(self.handle), "ctx_synchronize")
+
+    @property
+    def launch_count(self) -> int:
+        c = ctypes.c_uint64()
+        _check(_load().xpir_b200_ctx_launch_count(self.handle, ctypes.byref(c)), "ctx_launch_count")
+        return c.value
+
+    def import_db(self, elements, nb_elements: int, element_bytes: int, alpha: int, bits_per_coeff: int,
+                  element_stride: int | None = None) -> Database:
+        stride = element_bytes if element_stride is None else element_stride
+        h = ctypes.c_void_p()
+        _check(_load().xpir_b200_db_import(self.handle, _ptr(elements), nb_elements, element_bytes, stride, alpha,
+                                           bits_per_coeff, _on_device(elements), ctypes.byref(h)), "db_import")
+        return Database(self, h.value)
+
+    def reply(self, db: Database, n: list[int], query, out=None) -> np.ndarray:
+        """Reply of one query; `query` and `out` may be numpy (host) or torch CUDA tensors."""
+        d = len(n)
+        narr = (ctypes.c_uint32 * d)(*n)
+        Pl = db.polys_per_element
+        for _ in range(d - 1):
+            Pl = polys_per_element(Pl * self.ct_words * 8, 1, db.bits_per_coeff, self.N)
+        if out is None:
+            out = np.empty(Pl * self.ct_words, dtype=np.uint64)
+        cap = out.nbytes if isinstance(out, np.ndarray) else out.numel() * out.element_size()
+        cnt = ctypes.c_uint64()
+        _check(_load().xpir_b200_reply(self.handle, db.handle, d, narr, _ptr(query), _on_device(query), _ptr(out),
+                                       cap, _on_device(out), ctypes.byref(cnt)), "reply")
+        assert cnt.value == Pl
+        return out
+
+    def close(self) -> None:
+        if self.handle:
+            _check(_load().xpir_b200_ctx_destroy(self.handle), "ctx_destroy")
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

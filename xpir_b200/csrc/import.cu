@@ -1,0 +1,214 @@
+// Database import on the GPU: aggregation, bit split, CRT, phi-twist and the lazy
+// decimation-in-frequency NTT, fused in one kernel per (aggregated element, poly, modulus).
+//
+// Reference path (crypto/NFLlib.cpp:375-401, 672-916; crypto/NFLlib.hpp:450-537, 597-608;
+// pir/replyGenerator/PIRReplyGeneratorNFL_internal.cpp:79-158).  The same kernel performs
+// the re-import of level replies between recursion levels (…NFL_internal.cpp:599-626):
+// the P reply ciphertexts of an element are one contiguous little-endian bit stream.
+//
+// HBM layout of the output: [element][poly][modulus][coefficient] u64, values in [0, 2p).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kernels.h"
+#include "modarith.cuh"
+
+namespace xpir {
+
+DevModuli make_dev_moduli(const ParamSet &ps) {
+  DevModuli d{};
+  for (uint32_t c = 0; c < ps.m; c++) {
+    d.p[c] = ps.mod[c].p;
+    d.shoup_k[c] = ps.mod[c].shoup_k;
+    d.shoup_delta[c] = ps.mod[c].shoup_delta;
+    for (int t = 0; t < 4; t++) {
+      d.crt[c][t] = ps.mod[c].crt[t];
+      d.crt_shoup[c][t] = ps.mod[c].crt_shoup[t];
+    }
+  }
+  return d;
+}
+
+namespace {
+
+constexpr int kImportThreads = 256;
+
+struct ImportShape {
+  uint32_t N, log_n, m, b, nsub;
+  uint64_t P;
+  uint64_t total_bytes;  // bytes of one aggregated element (alpha * element_bytes)
+  uint32_t stage_words;  // u64 words of staged input per poly
+};
+
+// Byte i of aggregated element s, following the reference's reused import buffer: a
+// short last group (r < alpha real elements) reads its last real slot r-1 and slots up
+// to alpha-2 as zeros, and slot alpha-1 as the previous group's last element (zeros for
+// the first group).  See oracle xo_aggregate and pir/dbhandlers/DBHandler.cpp:3-26.
+__device__ __forceinline__ uint8_t agg_byte(const AggSource &src, uint64_t s, uint64_t i, uint64_t real) {
+  const uint64_t slot = i / src.element_bytes, off = i - slot * src.element_bytes;
+  const uint64_t first = s * src.alpha;
+  uint64_t elem;
+  if (real == src.alpha) {
+    elem = first + slot;
+  } else if (slot + 1 < real) {
+    elem = first + slot;
+  } else if (slot + 1 == src.alpha) {
+    if (s == 0) return 0;
+    elem = first - 1;
+  } else {
+    return 0;
+  }
+  return src.base[elem * src.element_stride + off];
+}
+
+// Twiddle layers of the reference NTT: log2(N)-2 radix-2 layers (inputs/outputs in [0,2p)),
+// then the last two layers fused per group of four (crypto/NFLlib.hpp:470-535).
+__device__ void ntt_lazy_smem(uint64_t *s, const uint64_t *__restrict__ w, const uint64_t *__restrict__ ws,
+                              uint32_t N, uint32_t log_n, uint64_t p) {
+  const uint64_t p2 = p << 1;
+  uint32_t half = N >> 1;
+  for (uint32_t l = 0; l + 2 < log_n; ++l) {
+    __syncthreads();
+    const uint32_t lh = log_n - 1 - l;  // log2(half)
+    for (uint32_t t = threadIdx.x; t < (N >> 1); t += blockDim.x) {
+      const uint32_t i = t & (half - 1);
+      const uint32_t idx = ((t >> lh) << (lh + 1)) + i;
+      const uint64_t u0 = s[idx], u1 = s[idx + half];
+      uint64_t t0 = u0 + u1;
+      t0 = (t0 >= p2) ? t0 - p2 : t0;
+      const uint64_t t1 = u0 - u1 + p2;
+      s[idx] = t0;
+      s[idx + half] = shoup_lazy(t1, __ldg(w + i), __ldg(ws + i), p);
+    }
+    w += half;
+    ws += half;
+    half >>= 1;
+  }
+  __syncthreads();
+  const uint64_t w1 = __ldg(w + 1), w1s = __ldg(ws + 1);
+  for (uint32_t g = threadIdx.x; g < (N >> 2); g += blockDim.x) {
+    uint64_t *y = s + 4 * g;
+    const uint64_t u0 = y[0], u1 = y[1], u2 = y[2], u3 = y[3];
+    uint64_t v0 = u0 + u2;
+    v0 = (v0 >= p2) ? v0 - p2 : v0;
+    uint64_t v2 = u0 - u2;
+    v2 = ((int64_t)v2 < 0) ? v2 + p2 : v2;
+    uint64_t v1 = u1 + u3;
+    v1 = (v1 >= p2) ? v1 - p2 : v1;
+    const uint64_t v3 = shoup_lazy(u1 - u3 + p2, w1, w1s, p);
+    uint64_t z0 = v0 + v1;
+    z0 = (z0 >= p2) ? z0 - p2 : z0;
+    uint64_t z1 = v0 - v1;
+    z1 = ((int64_t)z1 < 0) ? z1 + p2 : z1;
+    uint64_t z2 = v2 + v3;
+    z2 = (z2 >= p2) ? z2 - p2 : z2;
+    uint64_t z3 = v2 - v3;
+    z3 = ((int64_t)z3 < 0) ? z3 + p2 : z3;
+    y[0] = z0;
+    y[1] = z1;
+    y[2] = z2;
+    y[3] = z3;
+  }
+  __syncthreads();
+}
+
+// nbits (<= 56) bits starting at bit `pos` of the staged little-endian words.
+__device__ __forceinline__ uint64_t staged_bits(const uint64_t *st, uint64_t pos, uint32_t nbits) {
+  const uint64_t w = pos >> 6;
+  const uint32_t sh = (uint32_t)(pos & 63);
+  uint64_t v = st[w] >> sh;
+  if (sh) v |= st[w + 1] << (64 - sh);
+  return v & ((1ull << nbits) - 1);
+}
+
+// grid: x = aggregated element * P + poly, y = modulus.  Dynamic smem: stage words, then N words.
+__global__ void __launch_bounds__(kImportThreads) import_kernel(const AggSource src, const ImportShape sh,
+                                                                const DevModuli dm,
+                                                                const uint64_t *__restrict__ tables,
+                                                                uint64_t *__restrict__ out) {
+  extern __shared__ __align__(16) uint64_t smem[];
+  uint64_t *stage = smem;
+  uint64_t *poly = smem + sh.stage_words;
+  const uint64_t s = blockIdx.x / sh.P, j = blockIdx.x - s * sh.P;
+  const uint32_t c = blockIdx.y;
+  const uint32_t N = sh.N;
+  const uint64_t p = dm.p[c];
+
+  // Stage the bytes of this poly's bit range, from an 8-byte aligned start.
+  const uint64_t bit0 = j * (uint64_t)N * sh.b;
+  const uint64_t byte0 = (bit0 >> 3) & ~7ull;
+  const uint64_t first = s * src.alpha;
+  const uint64_t real = (first + src.alpha <= src.nb_elements) ? src.alpha : src.nb_elements - first;
+  const bool flat = (real == src.alpha) && (src.alpha == 1 || src.element_stride == src.element_bytes);
+  const uint8_t *flat_base = src.base + first * src.element_stride;
+  const bool aligned = flat && ((((uintptr_t)flat_base) & 7) == 0);
+  for (uint32_t w = threadIdx.x; w < sh.stage_words; w += blockDim.x) {
+    const uint64_t bpos = byte0 + 8ull * w;
+    uint64_t v = 0;
+    if (bpos + 8 <= sh.total_bytes && aligned) {
+      v = *reinterpret_cast<const uint64_t *>(flat_base + bpos);
+    } else {
+      for (uint32_t q = 0; q < 8; q++) {
+        const uint64_t i = bpos + q;
+        if (i < sh.total_bytes) {
+          const uint8_t byte = flat ? flat_base[i] : agg_byte(src, s, i, real);
+          v |= (uint64_t)byte << (8 * q);
+        }
+      }
+    }
+    stage[w] = v;
+  }
+  __syncthreads();
+
+  // Coefficients: b <= 56 one chunk per coefficient; b > 56 sub-chunks of 56 bits
+  // combined per modulus as sum_t mulmod(s_t, 2^(56t)) without a final reduction.
+  const uint64_t *tab = tables + (uint64_t)c * kTableSlots * N;
+  const uint64_t *phi = tab + kPhi * N, *phi_s = tab + kPhiShoup * N;
+  const uint64_t rel0 = bit0 - 8 * byte0;
+  for (uint32_t k = threadIdx.x; k < N; k += blockDim.x) {
+    const uint64_t pos = rel0 + (uint64_t)k * sh.b;
+    uint64_t x;
+    if (sh.nsub == 1) {
+      x = staged_bits(stage, pos, sh.b);
+    } else {
+      x = 0;
+      for (uint32_t t = 0; t < sh.nsub; t++) {
+        const uint32_t sz = (t + 1 < sh.nsub) ? 56 : sh.b - 56 * (sh.nsub - 1);
+        const uint64_t sub = staged_bits(stage, pos + 56ull * t, sz);
+        x += shoup_mul(sub, dm.crt[c][t], dm.crt_shoup[c][t], p);
+      }
+    }
+    poly[k] = shoup_mul(x, __ldg(phi + k), __ldg(phi_s + k), p);
+  }
+  ntt_lazy_smem(poly, tab + kOmega * N, tab + kOmegaShoup * N, N, sh.log_n, p);
+
+  uint64_t *o = out + ((s * sh.P + j) * sh.m + c) * (uint64_t)N;
+  for (uint32_t k = threadIdx.x; k < N; k += blockDim.x) o[k] = poly[k];
+}
+
+}  // namespace
+
+cudaError_t launch_import(const AggSource &src, uint64_t groups, uint64_t P, const ParamSet &ps,
+                          const DevModuli &dm, const uint64_t *tables, uint64_t *out, cudaStream_t stream) {
+  if (groups == 0 || P == 0) return cudaSuccess;
+  ImportShape sh;
+  sh.N = ps.N;
+  sh.log_n = ps.log_n;
+  sh.m = ps.m;
+  sh.b = ps.b;
+  sh.nsub = (ps.b + 55) / 56;
+  sh.P = P;
+  sh.total_bytes = (uint64_t)src.alpha * src.element_bytes;
+  // bits of one poly plus the in-word offset, rounded up, plus one spare word for the
+  // two-word reads of staged_bits
+  sh.stage_words = (uint32_t)((64 + (uint64_t)ps.N * ps.b + 63) / 64 + 2);
+  const size_t smem = (size_t)(sh.stage_words + ps.N) * sizeof(uint64_t);
+  cudaError_t e = cudaFuncSetAttribute(import_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  if (groups * P > 0x7fffffffull) return cudaErrorInvalidValue;
+  dim3 grid((unsigned)(groups * P), ps.m);
+  import_kernel<<<grid, kImportThreads, smem, stream>>>(src, sh, dm, tables, out);
+  return cudaGetLastError();
+}
+
+}  // namespace xpir

@@ -1,0 +1,58 @@
+// Kernel launchers of the B200 reply engine (device code in import.cu / reply.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "params.h"
+
+namespace xpir {
+
+// A database viewed the way the reference reads it for import: nb_elements elements of
+// element_bytes bytes (element i at base + i*element_stride), grouped alpha at a time
+// into aggregated elements of alpha*element_bytes bytes.  The last group, when short,
+// follows DBHandler::readAggregatedStream's reused-buffer behaviour
+// (pir/dbhandlers/DBHandler.cpp:3-26).
+struct AggSource {
+  const uint8_t *base;
+  uint64_t nb_elements;
+  uint64_t element_bytes;
+  uint64_t element_stride;
+  uint32_t alpha;
+};
+
+// Per-modulus constants the device needs, by value.
+struct DevModuli {
+  uint64_t p[kMaxModuli];
+  uint64_t shoup_k[kMaxModuli];
+  uint64_t shoup_delta[kMaxModuli];
+  uint64_t crt[kMaxModuli][4];
+  uint64_t crt_shoup[kMaxModuli][4];
+};
+
+DevModuli make_dev_moduli(const ParamSet &ps);
+
+// Import: for every aggregated element s < groups and poly j < P, bit-split + CRT +
+// phi-twist + forward NTT into out[(s*P + j)][m][N].  groups = ceil(nb/alpha),
+// P = polys_for_bits(8*alpha*element_bytes, b, N).  `tables` is the device copy of the
+// ParamSet tables.  Returns a CUDA error code.
+cudaError_t launch_import(const AggSource &src, uint64_t groups, uint64_t P, const ParamSet &ps,
+                          const DevModuli &dm, const uint64_t *tables, uint64_t *out, cudaStream_t stream);
+
+// One recursion level of the reply (pir/replyGenerator/PIRReplyGeneratorNFL_internal.cpp:511-595):
+// for group g < n_groups and poly cp < P, the in-order lazy Shoup accumulation over the
+// n_i slots of the group; slot q reads DB element g*n_i + q, an all-zero element when
+// that index is >= n_real.  out: [n_groups][P][2][m][N].
+struct ReplyLevelArgs {
+  const uint64_t *db;     // [n_real][P][m][N]
+  uint64_t n_real;
+  uint64_t P;
+  uint64_t n_groups;
+  uint64_t n_i;
+  const uint64_t *query;  // [n_i][2][m][N]
+  uint64_t *out;
+};
+cudaError_t launch_reply_level(const ReplyLevelArgs &a, const ParamSet &ps, const DevModuli &dm,
+                               cudaStream_t stream, uint32_t *launches);
+
+}  // namespace xpir

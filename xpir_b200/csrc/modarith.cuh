@@ -1,0 +1,97 @@
+// Modular arithmetic of the NFLLWE path, shared by host and device code.
+//
+// Every function reproduces the exact bit pattern of the reference's lazy arithmetic
+// (values are NOT canonical residues; see crypto/NFLlib.hpp:238-321).  Nothing here may
+// "clean up" a value with a % p: the reply accumulators and NTT outputs are compared
+// bit for bit with XPIR's CPU results.
+#pragma once
+
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define XPIR_HD __host__ __device__ __forceinline__
+#else
+#define XPIR_HD inline
+#endif
+
+namespace xpir {
+
+constexpr uint32_t kMaxModuli = 17;
+constexpr uint32_t kMinPolyDegree = 512;   // crypto/NFLParams.cpp:43
+constexpr uint32_t kMaxPolyDegree = 8192;  // crypto/NFLParams.cpp:44
+constexpr uint32_t kModulusBits = 60;      // crypto/NFLParams.cpp:31
+
+// High 64 bits of a 64x64-bit product.
+XPIR_HD uint64_t mulhi(uint64_t a, uint64_t b) {
+#if defined(__CUDA_ARCH__)
+  return __umul64hi(a, b);
+#else
+  return (uint64_t)(((unsigned __int128)a * b) >> 64);
+#endif
+}
+
+// Shoup product without the final correction: x*y - floor(x*ys/2^64)*p (mod 2^64).
+// For ys = floor(y*2^64/p) and y < p the result lies in [0, 2p) for any 64-bit x.
+XPIR_HD uint64_t shoup_lazy(uint64_t x, uint64_t y, uint64_t ys, uint64_t p) {
+  return x * y - mulhi(x, ys) * p;
+}
+
+// mulmodShoup (crypto/NFLlib.hpp:282-289): the lazy product with one conditional
+// subtraction.
+XPIR_HD uint64_t shoup_mul(uint64_t x, uint64_t y, uint64_t ys, uint64_t p) {
+  uint64_t r = shoup_lazy(x, y, ys, p);
+  return r >= p ? r - p : r;
+}
+
+// mulandaddShoup (crypto/NFLlib.hpp:303-321): rop += x*y - q*p (mod 2^64), then at most
+// one subtraction of p.
+XPIR_HD uint64_t shoup_mac(uint64_t rop, uint64_t x, uint64_t y, uint64_t ys, uint64_t p) {
+  rop += shoup_lazy(x, y, ys, p);
+  return rop >= p ? rop - p : rop;
+}
+
+// Constants for computing the Shoup factor floor(y*2^64/p) of a query word without a
+// 128-by-64-bit division.  Write 2^64 = k*p + delta (k = floor(2^64/p)).  Then
+//   floor(y*2^64/p) = k*y + floor(y*delta/p).
+// With z = y*delta (< 2^96 for delta < 2^32) and p <= 2^61, q0 = floor(z/2^61) is at
+// most floor(z/p) and, when z*(2^61-p) < p*2^61, at least floor(z/p) - 1; the remainder
+// z - q0*p lies in [0, 2p) and decides between the two.  shoup_factor_ok() checks these
+// conditions for a modulus; all 17 XPIR moduli (p = 2^61 - i*2^14 + 1) satisfy them.
+struct ShoupConst {
+  uint64_t p;
+  uint64_t k;      // floor(2^64 / p)
+  uint64_t delta;  // 2^64 - k*p
+};
+
+inline bool shoup_factor_ok(uint64_t p) {
+  if (p == 0 || p > (1ULL << 61) || p <= (1ULL << 59)) return false;
+  unsigned __int128 two64 = (unsigned __int128)1 << 64;
+  uint64_t k = (uint64_t)(two64 / p);
+  unsigned __int128 delta = two64 - (unsigned __int128)k * p;
+  if (delta >= ((unsigned __int128)1 << 32)) return false;
+  // z < 2^64*delta, so z*(2^61-p) < p*2^61 holds for every z when
+  // 2^64*delta*(2^61-p) <= p*2^61, i.e. 8*delta*(2^61-p) <= p.
+  unsigned __int128 lhs = (unsigned __int128)8 * delta * ((1ULL << 61) - p);
+  return lhs <= (unsigned __int128)p;
+}
+
+inline ShoupConst make_shoup_const(uint64_t p) {
+  unsigned __int128 two64 = (unsigned __int128)1 << 64;
+  ShoupConst s;
+  s.p = p;
+  s.k = (uint64_t)(two64 / p);
+  s.delta = (uint64_t)(two64 - (unsigned __int128)s.k * p);
+  return s;
+}
+
+// floor(y * 2^64 / p) mod 2^64, exact for every 64-bit y (the reference truncates the
+// 128-bit quotient to 64 bits the same way, PIRReplyGeneratorNFL_internal.cpp:764).
+XPIR_HD uint64_t shoup_factor(uint64_t y, uint64_t p, uint64_t k, uint64_t delta) {
+  const uint64_t zlo = y * delta;
+  const uint64_t zhi = mulhi(y, delta);
+  const uint64_t q0 = (zhi << 3) | (zlo >> 61);
+  const uint64_t rem = zlo - q0 * p;
+  return k * y + q0 + (rem >= p ? 1 : 0);
+}
+
+}  // namespace xpir
