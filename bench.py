@@ -27,9 +27,7 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 from pathlib import Path
 
@@ -64,50 +62,63 @@ def measured_peaks() -> dict:
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled every 20 ms through NVML during
+    the timed region (read-only queries; no GPU setting is changed)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
 
-    def __init__(self, device: int):
-        self.device = device
-        self.proc = None
-        self.tmp = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+    def __init__(self, device: int, interval_s: float = 0.02):
+        self.device, self.interval = device, interval_s
+        self.samples: list[tuple[float, int]] = []
+        self.max_mhz = None
+        self._stop = None
+        self._thread = None
+
+    def _run(self, nvml, handle):
+        while not self._stop.is_set():
+            try:
+                mhz = nvml.nvmlDeviceGetClockInfo(handle, nvml.NVML_CLOCK_SM)
+                reasons = nvml.nvmlDeviceGetCurrentClocksEventReasons(handle)
+                self.samples.append((float(mhz), int(reasons)))
+            except Exception:
+                pass
+            self._stop.wait(self.interval)
 
     def __enter__(self):
+        import threading
+
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.device)], stdout=self.tmp,
-                                         stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
+            import pynvml as nvml
+
+            nvml.nvmlInit()
+            # NVML enumerates all GPUs; map the CUDA ordinal through the visible-device list.
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            idx = int(vis.split(",")[self.device]) if vis and vis.split(",")[0].isdigit() else self.device
+            handle = nvml.nvmlDeviceGetHandleByIndex(idx)
+            self.max_mhz = float(nvml.nvmlDeviceGetMaxClockInfo(handle, nvml.NVML_CLOCK_SM))
+            self._stop = threading.Event()
+            self._thread = threading.Thread(target=self._run, args=(nvml, handle), daemon=True)
+            self._thread.start()
+        except Exception:
+            self._thread = None
         return self
 
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=2)
 
     def summary(self) -> dict:
-        self.tmp.flush()
-        rows = []
-        for line in Path(self.tmp.name).read_text().splitlines():
-            f = [x.strip() for x in line.split(",")]
-            if len(f) >= 9:
-                rows.append(f)
-        os.unlink(self.tmp.name)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": reasons, "samples": len(rows)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unavailable"], "samples": 0}
+        mhz = [s[0] for s in self.samples]
+        seen = 0
+        for _, r in self.samples:
+            seen |= r
+        reasons = sorted(name for name, bit in self.REASONS.items() if seen & bit)
+        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(self.samples)}
 
 
 def dist_setup():

@@ -37,6 +37,7 @@ extern "C" {
 #define XPIR_B200_ERR_CUDA (-3)    /* CUDA runtime error (see xpir_b200_last_cuda_error) */
 #define XPIR_B200_ERR_NODEV (-4)   /* no usable CUDA device */
 #define XPIR_B200_ERR_STATE (-5)   /* call out of order (e.g. incomplete query) */
+#define XPIR_B200_ERR_TIMEOUT (-6) /* a kernel's bounded wait expired; outputs are invalid */
 #define XPIR_B200_MAX_LEVELS 10    /* MAX_REC_LVL, pir/PIRParameters.hpp:22 */
 
 typedef struct xpir_b200_ctx xpir_b200_ctx; /* one (N, moduli) parameter set on one GPU */

@@ -21,11 +21,16 @@ int main() {
     const xpir::ShoupConst s = xpir::make_shoup_const(p);
     const uint64_t edge[] = {0, 1, 2, p - 2, p - 1, p, p + 1, 2 * p - 1, 2 * p, 3 * p + 7, (1ULL << 61) - 1,
                              1ULL << 61, (1ULL << 62) + 3, 1ULL << 63, ~0ULL - 1, ~0ULL};
+    if (!xpir::shoup_factor8_ok(p)) {
+      printf("modulus %u has no k=8 fast path\n", c);
+      return 1;
+    }
     auto check = [&](uint64_t y) {
       const uint64_t want = (uint64_t)(((unsigned __int128)y << 64) / p);
       const uint64_t got = xpir::shoup_factor(y, p, s.k, s.delta);
+      const uint64_t got8 = xpir::shoup_factor8(y, p, (uint32_t)s.delta);
       checked++;
-      if (want != got) {
+      if (want != got || want != got8) {
         printf("mismatch p=%llu y=%llu want=%llu got=%llu\n", (unsigned long long)p, (unsigned long long)y,
                (unsigned long long)want, (unsigned long long)got);
         exit(1);

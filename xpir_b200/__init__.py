@@ -25,6 +25,7 @@ ERR_NOMEM = -2
 ERR_CUDA = -3
 ERR_NODEV = -4
 ERR_STATE = -5
+ERR_TIMEOUT = -6
 
 _lib = None
 

@@ -30,6 +30,8 @@ struct xpir_b200_ctx {
   size_t ws_a_bytes = 0;
   void *ws_b = nullptr;  // re-imported level databases
   size_t ws_b_bytes = 0;
+  int *status_host = nullptr;  // kernel status word (mapped pinned memory)
+  int *status_dev = nullptr;
 };
 
 struct xpir_b200_db {
@@ -100,6 +102,7 @@ const char *xpir_b200_strerror(int status) {
     case XPIR_B200_ERR_CUDA: return "CUDA runtime error";
     case XPIR_B200_ERR_NODEV: return "no usable CUDA device";
     case XPIR_B200_ERR_STATE: return "call out of order";
+    case XPIR_B200_ERR_TIMEOUT: return "a device-side bounded wait expired";
     default: return "unknown status";
   }
 }
@@ -159,6 +162,11 @@ int xpir_b200_ctx_create(xpir_b200_ctx **out, int device, uint32_t N, uint32_t m
   if (rc == XPIR_B200_OK)
     rc = cuda_status(cudaMemcpy(ctx->d_tables, tables.data(), tables.size() * sizeof(uint64_t),
                                 cudaMemcpyHostToDevice));
+  if (rc == XPIR_B200_OK) rc = cuda_status(cudaHostAlloc(&ctx->status_host, sizeof(int), cudaHostAllocMapped));
+  if (rc == XPIR_B200_OK) {
+    *ctx->status_host = 0;
+    rc = cuda_status(cudaHostGetDevicePointer((void **)&ctx->status_dev, ctx->status_host, 0));
+  }
   if (rc != XPIR_B200_OK) {
     xpir_b200_ctx_destroy(ctx);
     return rc;
@@ -175,6 +183,7 @@ int xpir_b200_ctx_destroy(xpir_b200_ctx *ctx) {
   cudaFree(ctx->ws_query);
   cudaFree(ctx->ws_a);
   cudaFree(ctx->ws_b);
+  if (ctx->status_host) cudaFreeHost(ctx->status_host);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return XPIR_B200_OK;
@@ -336,12 +345,15 @@ int xpir_b200_reply(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, cons
 
   const uint64_t *in = db->d_polys;
   uint64_t in_real = db->n_agg;
+  *ctx->status_host = 0;
   for (uint32_t lvl = 0; lvl < d; lvl++) {
     const bool last = lvl + 1 == d;
     uint64_t *rep = (last && out_on_device) ? (uint64_t *)replies : (uint64_t *)ctx->ws_a;
     uint32_t launched = 0;
     ReplyLevelArgs a{in, in_real, Ps[lvl], groups[lvl], n[lvl], dq, rep};
-    XPIR_TRY(launch_reply_level(a, ps, dm, ctx->stream, &launched));
+    const cudaError_t le = launch_reply_level(a, ps, dm, ctx->stream, &launched, ctx->status_dev);
+    if (le == cudaErrorNotSupported) return XPIR_B200_ERR_ARG;
+    XPIR_TRY(le);
     ctx->launches += launched;
     dq += (uint64_t)n[lvl] * ct_words;
     if (last) break;
@@ -357,6 +369,7 @@ int xpir_b200_reply(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, cons
   if (!out_on_device)
     XPIR_TRY(cudaMemcpyAsync(replies, ctx->ws_a, final_bytes, cudaMemcpyDeviceToHost, ctx->stream));
   XPIR_TRY(cudaStreamSynchronize(ctx->stream));
+  if (*(volatile int *)ctx->status_host != 0) return XPIR_B200_ERR_TIMEOUT;
   if (nb_replies) *nb_replies = final_count;
   return XPIR_B200_OK;
 }

@@ -52,7 +52,13 @@ struct ReplyLevelArgs {
   const uint64_t *query;  // [n_i][2][m][N]
   uint64_t *out;
 };
+// `status` is a device-visible int that a kernel sets to a nonzero KernelStatus when one
+// of its bounded waits gives up (sm100.cuh); the caller clears and reads it.
 cudaError_t launch_reply_level(const ReplyLevelArgs &a, const ParamSet &ps, const DevModuli &dm,
-                               cudaStream_t stream, uint32_t *launches);
+                               cudaStream_t stream, uint32_t *launches, int *status);
+
+// Whether the reply kernel supports this level shape (moduli with the fast Shoup-factor
+// path, degree a multiple of the slice width, 32-bit TMA coordinates).
+bool reply_level_supported(const ParamSet &ps, uint64_t n_real, uint64_t n_i, uint64_t groups);
 
 }  // namespace xpir

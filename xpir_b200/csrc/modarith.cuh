@@ -94,4 +94,25 @@ XPIR_HD uint64_t shoup_factor(uint64_t y, uint64_t p, uint64_t k, uint64_t delta
   return k * y + q0 + (rem >= p ? 1 : 0);
 }
 
+// The same factor for moduli with k = 8 and delta < 2^26 (all 17 XPIR moduli), from
+// 32x32-bit partial products only.  With y = yh*2^32 + yl:
+//   A = yl*delta < 2^58,  B = yh*delta < 2^58,  z = y*delta = B*2^32 + A < 2^90,
+//   q0 = floor(z / 2^61) = floor((B + floor(A/2^32)) / 2^29) < 2^30,
+// and z mod 2^64 = A + B*2^32 (mod 2^64).  The remainder z - q0*p is in [0, 2p) (see
+// shoup_factor_ok), so floor(z/p) = q0 + [z - q0*p >= p].
+inline bool shoup_factor8_ok(uint64_t p) {
+  if (!shoup_factor_ok(p)) return false;
+  const ShoupConst s = make_shoup_const(p);
+  return s.k == 8 && s.delta < (1ull << 26);
+}
+
+XPIR_HD uint64_t shoup_factor8(uint64_t y, uint64_t p, uint32_t delta) {
+  const uint64_t A = (uint64_t)(uint32_t)y * delta;
+  const uint64_t B = (uint64_t)(uint32_t)(y >> 32) * delta;
+  const uint32_t q0 = (uint32_t)((B + (A >> 32)) >> 29);
+  const uint64_t zlo = A + (B << 32);
+  const uint64_t rem = zlo - (uint64_t)q0 * p;
+  return (y << 3) + q0 + (rem >= p ? 1u : 0u);
+}
+
 }  // namespace xpir
