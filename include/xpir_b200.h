@@ -74,6 +74,8 @@ XPIR_B200_API uint64_t xpir_b200_ciphertext_bytes(uint32_t poly_degree, uint32_t
  * the role of NFLlib::setNewParameters/configureNTT (crypto/NFLlib.cpp:44-228).  The
  * context owns one CUDA stream; all its work is ordered on it. */
 XPIR_B200_API int xpir_b200_ctx_create(xpir_b200_ctx **ctx, int device, uint32_t poly_degree, uint32_t nb_moduli);
+/* Destroys the context and every database imported through it (their handles become
+ * invalid and must not be passed to xpir_b200_db_free afterwards). */
 XPIR_B200_API int xpir_b200_ctx_destroy(xpir_b200_ctx *ctx);
 /* The context's cudaStream_t, as a void pointer (for event timing by the caller). */
 XPIR_B200_API int xpir_b200_ctx_stream(xpir_b200_ctx *ctx, void **stream);

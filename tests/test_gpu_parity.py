@@ -154,3 +154,16 @@ def test_launch_count_and_reuse(engine, oracle):
             rep = ctx.reply(d, n, q)
             assert np.array_equal(rep, oracle.reply(imp, F, P, n, q, b, N, m))
         assert ctx.launch_count - before == 3 * 3  # per reply: 2 level kernels + 1 re-import
+
+
+def test_context_close_releases_databases(engine, oracle):
+    """Closing a context frees the databases imported through it; freeing such a
+    database afterwards (explicitly or by garbage collection) is harmless."""
+    ctx = engine.Context(1024, 1)
+    d = ctx.import_db(random_db(41, 10, 500), 10, 500, 1, oracle.bits_per_coeff(1024, 1, 10))
+    ctx.close()
+    d.free()
+    del d
+    with engine.Context(1024, 1) as ctx2:
+        d2 = ctx2.import_db(random_db(42, 10, 500), 10, 500, 1, oracle.bits_per_coeff(1024, 1, 10))
+    del d2

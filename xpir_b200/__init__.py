@@ -12,6 +12,7 @@ HBM (XPIR's ``imported_database``), and :meth:`Context.reply` is
 from __future__ import annotations
 
 import ctypes
+import weakref
 from pathlib import Path
 
 import numpy as np
@@ -157,9 +158,10 @@ class Database:
         return out
 
     def free(self) -> None:
-        if self.handle:
+        # A closed context has already released its databases.
+        if self.handle and self.ctx.handle:
             _check(_load().xpir_b200_db_free(self.handle), "db_free")
-            self.handle = None
+        self.handle = None
 
     def __del__(self):
         try:
@@ -177,6 +179,7 @@ class Context:
         _check(_load().xpir_b200_ctx_create(ctypes.byref(h), device, N, m), "ctx_create")
         self.handle = h
         self.ct_words = 2 * m * N
+        self._dbs: "weakref.WeakSet[Database]" = weakref.WeakSet()
 
     @property
     def stream(self) -> int:
@@ -199,7 +202,9 @@ class Context:
         h = ctypes.c_void_p()
         _check(_load().xpir_b200_db_import(self.handle, _ptr(elements), nb_elements, element_bytes, stride, alpha,
                                            bits_per_coeff, _on_device(elements), ctypes.byref(h)), "db_import")
-        return Database(self, h.value)
+        db = Database(self, h.value)
+        self._dbs.add(db)
+        return db
 
     def reply(self, db: Database, n: list[int], query, out=None) -> np.ndarray:
         """Reply of one query; `query` and `out` may be numpy (host) or torch CUDA tensors."""
@@ -219,6 +224,8 @@ class Context:
 
     def close(self) -> None:
         if self.handle:
+            for db in list(self._dbs):
+                db.free()
             _check(_load().xpir_b200_ctx_destroy(self.handle), "ctx_destroy")
             self.handle = None
 

@@ -8,9 +8,10 @@
 #include <string.h>
 
 #include <mutex>
+#include <set>
 #include <vector>
 
-#include "../../include/xpir_b200.h"
+#include "xpir_b200.h"
 #include "kernels.h"
 #include "params.h"
 
@@ -32,6 +33,7 @@ struct xpir_b200_ctx {
   size_t ws_b_bytes = 0;
   int *status_host = nullptr;  // kernel status word (mapped pinned memory)
   int *status_dev = nullptr;
+  std::set<xpir_b200_db *> dbs;  // databases imported through this context
 };
 
 struct xpir_b200_db {
@@ -179,6 +181,11 @@ int xpir_b200_ctx_destroy(xpir_b200_ctx *ctx) {
   if (!ctx) return XPIR_B200_ERR_ARG;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (xpir_b200_db *db : ctx->dbs) {
+    cudaFree(db->d_polys);
+    delete db;
+  }
+  ctx->dbs.clear();
   cudaFree(ctx->d_tables);
   cudaFree(ctx->ws_query);
   cudaFree(ctx->ws_a);
@@ -260,14 +267,18 @@ int xpir_b200_db_import(xpir_b200_ctx *ctx, const void *elements, uint64_t nb_el
     delete db;
     return cuda_status(e);
   }
+  ctx->dbs.insert(db);
   *out = db;
   return XPIR_B200_OK;
 }
 
 int xpir_b200_db_free(xpir_b200_db *db) {
   if (!db) return XPIR_B200_ERR_ARG;
-  cudaSetDevice(db->ctx->device);
-  cudaStreamSynchronize(db->ctx->stream);
+  xpir_b200_ctx *ctx = db->ctx;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  if (!ctx->dbs.erase(db)) return XPIR_B200_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
   cudaFree(db->d_polys);
   delete db;
   return XPIR_B200_OK;

@@ -34,37 +34,66 @@
 #include "modarith.cuh"
 #include "sm100.cuh"
 
+// Single-column shape, chosen by a timing sweep on B200 over W in {8, 16, 32}, E in
+// {16..128}, NS in {2..8}, term buffers in {2, 4, 8} (the 100k x 4 KB workload).
+#ifndef XPIR_P1_W
+#define XPIR_P1_W 16
+#define XPIR_P1_E 64
+#define XPIR_P1_NS 3
+#define XPIR_P1_TB 2
+#endif
+
 namespace xpir {
 namespace {
 
-constexpr int kW = 16;              // coefficients per slice (128-byte TMA rows)
-constexpr int kComputeWarps = 8;
-constexpr int kComputeThreads = 32 * kComputeWarps;
+// Tile configuration: W coefficients per slice, C poly columns, E slots per tile, NS
+// pipeline stages.  One compute thread per slot pair of the tile; one chain thread per
+// (half, column, coefficient).
+template <int W, int C, int E, int NS, int TB = 2>
+struct Cfg {
+  static constexpr int kComputeWarps = E * W / 2 / 32;
+  static constexpr int kComputeThreads = 32 * kComputeWarps;
+  static constexpr int kChainThreads = 2 * C * W;
+  static constexpr int kChainWarps = (kChainThreads + 31) / 32;
+  static constexpr int kThreads = 32 * (1 + kComputeWarps + kChainWarps);
+  static constexpr int kX = E * C * W;     // DB box    [E][C][W]
+  static constexpr int kQ = E * 2 * W;     // query box [E][2][W]
+  static constexpr int kT = 2 * C * E * W;  // terms     [half][C][E/2][W][2] per buffer
+  static constexpr size_t kBytes = (size_t)(NS * (kX + kQ) + TB * kT) * 8 + (2 * NS + 2 * TB) * 8;
+  static_assert((TB & (TB - 1)) == 0, "term buffers: a power of two");
+  static_assert(E % 2 == 0 && (E * W / 2) % 32 == 0, "slot pairs must fill whole warps");
+  static_assert((W * 8) % 16 == 0, "TMA rows must be multiples of 16 bytes");
+};
+
+// 16-byte shared-memory load/store of two consecutive words.  volatile keeps a batch of
+// loads where it is written, ahead of the arithmetic that consumes the previous batch.
+__device__ __forceinline__ void lds_v2(const uint64_t *p, uint64_t &a, uint64_t &b) {
+  asm volatile("ld.shared.v2.u64 {%0, %1}, [%2];\n" : "=l"(a), "=l"(b) : "r"(smem_addr(p)) : "memory");
+}
+__device__ __forceinline__ void sts_v2(uint64_t *p, uint64_t a, uint64_t b) {
+  asm volatile("st.shared.v2.u64 [%0], {%1, %2};\n" ::"r"(smem_addr(p)), "l"(a), "l"(b) : "memory");
+}
 
 struct LevelShape {
   uint64_t n_real, P, n_i;
   uint32_t N, m, col_blocks;
 };
 
-template <int C, int E, int NS>
-struct Smem {
-  static constexpr int kX = E * C * kW;     // DB box  [E][C][W]
-  static constexpr int kQ = E * 2 * kW;     // query box [E][2][W]
-  static constexpr int kT = 2 * C * E * kW;  // terms [half][C][E][W] per buffer
-  static constexpr size_t kBytes = (size_t)(NS * (kX + kQ) + 2 * kT) * 8 + (2 * NS + 4) * 8;
-};
 
-template <int C, int E, int NS>
-__global__ void __launch_bounds__(32 + kComputeThreads + 32 * C, C <= 2 ? 2 : 1)
+template <int W, int C, int E, int NS, int TB>
+__global__ void __launch_bounds__(Cfg<W, C, E, NS, TB>::kThreads, C <= 2 ? 2 : 1)
     reply_tma_kernel(const __grid_constant__ CUtensorMap tm_db, const __grid_constant__ CUtensorMap tm_q,
                      uint64_t *__restrict__ out, const LevelShape sh, const DevModuli dm, int *status) {
-  using S = Smem<C, E, NS>;
+  using S = Cfg<W, C, E, NS, TB>;
+  constexpr int kComputeWarps = S::kComputeWarps;
+  constexpr int kComputeThreads = S::kComputeThreads;
+  constexpr int kW = W;
   extern __shared__ __align__(128) uint64_t sm[];
   uint64_t *xs = sm;                         // [NS][E][C][W]
   uint64_t *qs = xs + NS * S::kX;            // [NS][E][2][W]
-  uint64_t *terms = qs + NS * S::kQ;         // [2][2][C][E][W]
-  uint64_t *bars = terms + 2 * S::kT;
-  uint64_t *full = bars, *empty = bars + NS, *tfull = bars + 2 * NS, *tempty = bars + 2 * NS + 2;
+  uint64_t *terms = qs + NS * S::kQ;         // [TB][2][C][E/2][W][2]
+  uint64_t *bars = terms + TB * S::kT;
+  uint64_t *full = bars, *empty = bars + NS, *tfull = bars + 2 * NS, *tempty = bars + 2 * NS + TB;
 
   const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const uint64_t g = blockIdx.x;
@@ -73,7 +102,7 @@ __global__ void __launch_bounds__(32 + kComputeThreads + 32 * C, C <= 2 ? 2 : 1)
   const uint32_t cp0 = (blockIdx.z - c * sh.col_blocks) * C;
   const uint64_t p = dm.p[c];
   const uint32_t delta = (uint32_t)dm.shoup_delta[c];
-  const uint64_t tiles = (sh.n_i + E - 1) / E;
+  const uint32_t tiles = (uint32_t)((sh.n_i + E - 1) / E);
 
   if (threadIdx.x == 0) {
     // Every consumer thread arrives on the release barriers, so each thread's own
@@ -82,9 +111,9 @@ __global__ void __launch_bounds__(32 + kComputeThreads + 32 * C, C <= 2 ? 2 : 1)
       mbar_init(full + s, 1);
       mbar_init(empty + s, kComputeThreads);
     }
-    for (int b = 0; b < 2; b++) {
+    for (int b = 0; b < TB; b++) {
       mbar_init(tfull + b, kComputeThreads);
-      mbar_init(tempty + b, 32 * C);
+      mbar_init(tempty + b, S::kChainThreads);
     }
     mbar_fence_init();
   }
@@ -97,46 +126,49 @@ __global__ void __launch_bounds__(32 + kComputeThreads + 32 * C, C <= 2 ? 2 : 1)
       tma_prefetch_desc(&tm_db);
       tma_prefetch_desc(&tm_q);
       constexpr uint32_t kTx = (uint32_t)((S::kX + S::kQ) * 8);
-      uint64_t t = 0;
+      uint32_t t = 0;
       for (; t < tiles; ++t) {
         const int s = (int)(t % NS);
-        if (t >= (uint64_t)NS && !mbar_wait(empty + s, (uint32_t)((t / NS - 1) & 1))) {
+        if (t >= (uint32_t)NS && !mbar_wait(empty + s, (t / NS - 1) & 1)) {
           ok = false;
           break;
         }
         mbar_arrive_expect_tx(full + s, kTx);
-        const int slot = (int)(t * E);
+        const int slot = (int)t * E;
         tma_load_4d(xs + s * S::kX, &tm_db, k0, (int)c, (int)cp0, (int)(g * sh.n_i) + slot, full + s);
         tma_load_4d(qs + s * S::kQ, &tm_q, k0, (int)c, 0, slot, full + s);
       }
       // Drain: every issued copy must have landed before the CTA exits.
-      const uint64_t first = t > (uint64_t)NS ? t - NS : 0;
-      for (uint64_t u = first; u < t; ++u) mbar_wait(full + (u % NS), (uint32_t)((u / NS) & 1));
+      const uint32_t first = t > (uint32_t)NS ? t - NS : 0;
+      for (uint32_t u = first; u < t; ++u) mbar_wait(full + (u % NS), (u / NS) & 1);
     }
   } else if (warp <= kComputeWarps) {
     // ---- compute warps: query Shoup factors and terms -------------------------------
     const int ct = threadIdx.x - 32;
-    for (uint64_t t = 0; t < tiles && ok; ++t) {
-      const int s = (int)(t % NS), b = (int)(t & 1);
-      if (!mbar_wait(full + s, (uint32_t)((t / NS) & 1))) ok = false;
-      if (ok && t >= 2 && !mbar_wait(tempty + b, (uint32_t)((t / 2 - 1) & 1))) ok = false;
+    for (uint32_t t = 0; t < tiles && ok; ++t) {
+      const int s = (int)(t % NS), b = (int)(t % TB);
+      if (!mbar_wait(full + s, (t / NS) & 1)) ok = false;
+      if (ok && t >= (uint32_t)TB && !mbar_wait(tempty + b, (t / TB - 1) & 1)) ok = false;
       if (!ok) break;
       const uint64_t *xst = xs + s * S::kX;
       const uint64_t *qst = qs + s * S::kQ;
       uint64_t *tb = terms + b * S::kT;
-#pragma unroll
-      for (int r = 0; r < (E * kW) / kComputeThreads; r++) {
-        const int item = ct + r * kComputeThreads;
-        const int e = item / kW, k = item % kW;
-        const uint64_t ya = qst[(e * 2 + 0) * kW + k];
-        const uint64_t yb = qst[(e * 2 + 1) * kW + k];
-        const uint64_t ysa = shoup_factor8(ya, p, delta);
-        const uint64_t ysb = shoup_factor8(yb, p, delta);
+      // Thread -> (coefficient k, slot pair e, e+1); the pair is stored as one 16-byte
+      // word so that a chain thread reads two consecutive slots with one load.
+      {
+        const int item = ct;
+        const int k = item % kW, ep = item / kW, e = 2 * ep;
+        const uint64_t ya0 = qst[(e * 2 + 0) * kW + k], yb0 = qst[(e * 2 + 1) * kW + k];
+        const uint64_t ya1 = qst[(e * 2 + 2) * kW + k], yb1 = qst[(e * 2 + 3) * kW + k];
+        const uint64_t ysa0 = shoup_factor8(ya0, p, delta), ysb0 = shoup_factor8(yb0, p, delta);
+        const uint64_t ysa1 = shoup_factor8(ya1, p, delta), ysb1 = shoup_factor8(yb1, p, delta);
 #pragma unroll
         for (int col = 0; col < C; col++) {
-          const uint64_t x = xst[(e * C + col) * kW + k];
-          tb[((0 * C + col) * E + e) * kW + k] = shoup_lazy(x, ya, ysa, p);
-          tb[((1 * C + col) * E + e) * kW + k] = shoup_lazy(x, yb, ysb, p);
+          const uint64_t x0 = xst[(e * C + col) * kW + k], x1 = xst[((e + 1) * C + col) * kW + k];
+          sts_v2(tb + (((0 * C + col) * (E / 2) + ep) * kW + k) * 2, shoup_lazy(x0, ya0, ysa0, p),
+                 shoup_lazy(x1, ya1, ysa1, p));
+          sts_v2(tb + (((1 * C + col) * (E / 2) + ep) * kW + k) * 2, shoup_lazy(x0, yb0, ysb0, p),
+                 shoup_lazy(x1, yb1, ysb1, p));
         }
       }
       mbar_arrive(empty + s);
@@ -145,40 +177,42 @@ __global__ void __launch_bounds__(32 + kComputeThreads + 32 * C, C <= 2 ? 2 : 1)
   } else {
     // ---- chain warps: strictly in-order accumulation ---------------------------------
     const int u = threadIdx.x - 32 - kComputeThreads;  // (half, column, coefficient)
+    if (u >= S::kChainThreads) return;
     const int h = u / (C * kW), col = (u / kW) % C, k = u % kW;
     uint64_t rop = 0;
-    for (uint64_t t = 0; t < tiles; ++t) {
-      const int b = (int)(t & 1);
-      if (!mbar_wait(tfull + b, (uint32_t)((t / 2) & 1))) {
+    for (uint32_t t = 0; t < tiles; ++t) {
+      const int b = (int)(t % TB);
+      if (!mbar_wait(tfull + b, (t / TB) & 1)) {
         ok = false;
         break;
       }
-      const uint64_t *tb = terms + b * S::kT + ((h * C + col) * E) * kW + k;
-      const uint64_t left = sh.n_i - t * E;
+      const uint64_t *tb = terms + b * S::kT + ((h * C + col) * (E / 2) * kW + k) * 2;
+      const uint64_t left = sh.n_i - (uint64_t)t * E;
       if (left >= (uint64_t)E) {
-        // Loads are issued a batch ahead of the dependent add/compare/subtract so that
-        // only the 64-bit chain arithmetic is on the critical path.
-        constexpr int kB = 8;
-        uint64_t cur[kB], nxt[kB];
+        // Terms come in batches of kB slot pairs; batch i+1 is requested before batch i
+        // is accumulated, so only the 64-bit add/compare/subtract is on the serial path.
+        constexpr int kB = 4;
+        static_assert((E / 2) % kB == 0, "batches must divide the tile");
+        uint64_t cur[2 * kB], nxt[2 * kB];
 #pragma unroll
-        for (int j = 0; j < kB; j++) cur[j] = tb[j * kW];
+        for (int j = 0; j < kB; j++) lds_v2(tb + j * kW * 2, cur[2 * j], cur[2 * j + 1]);
 #pragma unroll
-        for (int e0 = 0; e0 < E; e0 += kB) {
-          if (e0 + kB < E) {
+        for (int e0 = 0; e0 < E / 2; e0 += kB) {
+          if (e0 + kB < E / 2) {
 #pragma unroll
-            for (int j = 0; j < kB; j++) nxt[j] = tb[(e0 + kB + j) * kW];
+            for (int j = 0; j < kB; j++) lds_v2(tb + (e0 + kB + j) * kW * 2, nxt[2 * j], nxt[2 * j + 1]);
           }
 #pragma unroll
-          for (int j = 0; j < kB; j++) {
+          for (int j = 0; j < 2 * kB; j++) {
             const uint64_t w = rop + cur[j];
             rop = w >= p ? w - p : w;
           }
 #pragma unroll
-          for (int j = 0; j < kB; j++) cur[j] = nxt[j];
+          for (int j = 0; j < 2 * kB; j++) cur[j] = nxt[j];
         }
       } else {
         for (int e = 0; e < (int)left; e++) {
-          const uint64_t w = rop + tb[e * kW];
+          const uint64_t w = rop + tb[((e / 2) * kW) * 2 + (e & 1)];
           rop = w >= p ? w - p : w;
         }
       }
@@ -196,7 +230,7 @@ __global__ void __launch_bounds__(32 + kComputeThreads + 32 * C, C <= 2 ? 2 : 1)
   }
 }
 
-template <int C, int E, int NS>
+template <int W, int C, int E, int NS, int TB = 2>
 cudaError_t launch_c(const ReplyLevelArgs &a, const ParamSet &ps, const DevModuli &dm, uint64_t groups,
                      cudaStream_t stream, int *status) {
   // DB level viewed as [element][poly][modulus][coefficient]; query as [slot][half][modulus][coefficient].
@@ -204,22 +238,22 @@ cudaError_t launch_c(const ReplyLevelArgs &a, const ParamSet &ps, const DevModul
   CUtensorMap tm_db, tm_q;
   const uint64_t db_dims[4] = {N, m, a.P, a.n_real};
   const uint64_t db_strides[3] = {N * 8, m * N * 8, a.P * m * N * 8};
-  const uint32_t db_box[4] = {(uint32_t)kW, 1, (uint32_t)C, (uint32_t)E};
+  const uint32_t db_box[4] = {(uint32_t)W, 1, (uint32_t)C, (uint32_t)E};
   const uint64_t q_dims[4] = {N, m, 2, a.n_i};
   const uint64_t q_strides[3] = {N * 8, m * N * 8, 2 * m * N * 8};
-  const uint32_t q_box[4] = {(uint32_t)kW, 1, 2, (uint32_t)E};
+  const uint32_t q_box[4] = {(uint32_t)W, 1, 2, (uint32_t)E};
   if (!encode_tensor_map_u64_4d(&tm_db, a.db, db_dims, db_strides, db_box) ||
       !encode_tensor_map_u64_4d(&tm_q, a.query, q_dims, q_strides, q_box))
     return cudaErrorInvalidValue;
-  using S = Smem<C, E, NS>;
-  auto kern = reply_tma_kernel<C, E, NS>;
+  using S = Cfg<W, C, E, NS, TB>;
+  auto kern = reply_tma_kernel<W, C, E, NS, TB>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kBytes);
   if (e != cudaSuccess) return e;
   const uint32_t col_blocks = (uint32_t)((a.P + C - 1) / C);
   LevelShape sh{a.n_real, a.P, a.n_i, ps.N, ps.m, col_blocks};
   if (groups > 0x7fffffffull || (uint64_t)m * col_blocks > 65535) return cudaErrorInvalidValue;
-  dim3 grid((unsigned)groups, ps.N / kW, (unsigned)(m * col_blocks));
-  kern<<<grid, 32 + kComputeThreads + 32 * C, S::kBytes, stream>>>(tm_db, tm_q, a.out, sh, dm, status);
+  dim3 grid((unsigned)groups, ps.N / W, (unsigned)(m * col_blocks));
+  kern<<<grid, S::kThreads, S::kBytes, stream>>>(tm_db, tm_q, a.out, sh, dm, status);
   return cudaGetLastError();
 }
 
@@ -229,7 +263,7 @@ bool reply_level_supported(const ParamSet &ps, uint64_t n_real, uint64_t n_i, ui
   for (uint32_t c = 0; c < ps.m; c++)
     if (!shoup_factor8_ok(ps.mod[c].p)) return false;
   // TMA coordinates are 32-bit signed.
-  return ps.N % kW == 0 && n_real < (1ull << 31) && groups * n_i + 256 < (1ull << 31);
+  return ps.N % 16 == 0 && n_real < (1ull << 31) && groups * n_i + 256 < (1ull << 31);
 }
 
 cudaError_t launch_reply_level(const ReplyLevelArgs &a, const ParamSet &ps, const DevModuli &dm,
@@ -247,15 +281,16 @@ cudaError_t launch_reply_level(const ReplyLevelArgs &a, const ParamSet &ps, cons
   if (active == 0) return cudaSuccess;
   if (!reply_level_supported(ps, a.n_real, a.n_i, active)) return cudaErrorNotSupported;
   if (launches) (*launches)++;
+  // Tile shapes per poly-column count (W, C, E, NS[, term buffers]).
   switch (a.P) {
-    case 1: return launch_c<1, 32, 4>(a, ps, dm, active, stream, status);
-    case 2: return launch_c<2, 32, 3>(a, ps, dm, active, stream, status);
-    case 3: return launch_c<3, 16, 4>(a, ps, dm, active, stream, status);
-    case 4: return launch_c<4, 16, 3>(a, ps, dm, active, stream, status);
-    case 5: return launch_c<5, 16, 3>(a, ps, dm, active, stream, status);
-    case 6: return launch_c<6, 16, 3>(a, ps, dm, active, stream, status);
-    case 7: return launch_c<7, 16, 3>(a, ps, dm, active, stream, status);
-    default: return launch_c<8, 16, 3>(a, ps, dm, active, stream, status);
+    case 1: return launch_c<XPIR_P1_W, 1, XPIR_P1_E, XPIR_P1_NS, XPIR_P1_TB>(a, ps, dm, active, stream, status);
+    case 2: return launch_c<16, 2, 32, 3>(a, ps, dm, active, stream, status);
+    case 3: return launch_c<16, 3, 16, 4>(a, ps, dm, active, stream, status);
+    case 4: return launch_c<16, 4, 16, 3>(a, ps, dm, active, stream, status);
+    case 5: return launch_c<16, 5, 16, 3>(a, ps, dm, active, stream, status);
+    case 6: return launch_c<16, 6, 16, 3>(a, ps, dm, active, stream, status);
+    case 7: return launch_c<16, 7, 16, 3>(a, ps, dm, active, stream, status);
+    default: return launch_c<16, 8, 16, 3>(a, ps, dm, active, stream, status);
   }
 }
 

@@ -8,10 +8,12 @@
 
 namespace xpir {
 
-// Upper bound on try_wait polls of one mbarrier wait.  try_wait itself suspends the
-// thread for a hardware-defined interval between polls, so this bounds a wait to a few
-// seconds; past it the kernel records an error and returns instead of spinning forever.
-constexpr uint32_t kSpinLimit = 1u << 24;
+// Each try_wait poll may suspend the thread for up to kSuspendNs (it wakes as soon as the
+// phase completes), so a waiting warp costs almost no issue slots.  kSpinLimit polls bound
+// one wait to about kSpinLimit * kSuspendNs (~2.6 s); past it the kernel records an error
+// and returns instead of spinning forever.
+constexpr uint32_t kSuspendNs = 20000;
+constexpr uint32_t kSpinLimit = 1u << 17;
 
 // Error codes a kernel can leave in its status word.
 enum KernelStatus : int { kStatusOk = 0, kStatusWaitTimeout = 1 };
@@ -38,9 +40,9 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t by
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity)
+      : "r"(smem_addr(bar)), "r"(parity), "n"(kSuspendNs)
       : "memory");
   return ok != 0;
 }
