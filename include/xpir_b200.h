@@ -120,6 +120,33 @@ XPIR_B200_API int xpir_b200_reply(xpir_b200_ctx *ctx, const xpir_b200_db *db, ui
                     int query_on_device, void *replies, uint64_t capacity_bytes, int out_on_device,
                     uint64_t *nb_replies);
 
+/* ---- reply without allocation ---------------------------------------------------- */
+/* Bytes of device scratch available to xpir_b200_reply_noalloc (64 MiB). */
+#define XPIR_B200_NOALLOC_SCRATCH_BYTES (64ull << 20)
+/* No counterpart in the reference: an extra entry point of this library.
+ *
+ * Same result as xpir_b200_reply for a query and a reply buffer that are both already in
+ * device memory, but this call allocates nothing: no cudaMalloc, cudaFree or pinned
+ * buffer.  It is meant for callers that must not allocate while serving a request, for
+ * example a caller that has set up all its memory in advance under a fixed device-memory
+ * budget, or that runs inside an allocator or memory-pool hook of its own where a
+ * nested allocation is not allowed.  The intermediate data of a recursive query (the
+ * replies of each level and the next level's database) goes to one fixed scratch area
+ * of XPIR_B200_NOALLOC_SCRATCH_BYTES that the library holds in the global memory of
+ * every GPU that loads it, until the process exits.  A query whose intermediate data
+ * does not fit is rejected with XPIR_B200_ERR_ARG before anything is launched; a d = 1
+ * query uses no scratch.
+ *
+ * The first call on a device looks up that device's scratch address; make that first
+ * call before capturing a CUDA stream on it.  All calls share the one scratch area and it
+ * keeps the previous call's contents (every word a call reads there is written by the
+ * same call first): calls that overlap on the same GPU, from different threads or
+ * contexts, race with each other and must be serialised by the caller.  The context
+ * and the imported database are created beforehand with the allocating calls above. */
+XPIR_B200_API int xpir_b200_reply_noalloc(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, const uint32_t *n,
+                                          const void *query_dev, void *replies_dev, uint64_t capacity_bytes,
+                                          uint64_t *nb_replies);
+
 #ifdef __cplusplus
 }
 #endif
