@@ -299,11 +299,11 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
         if algo_bytes:
             achieved = algo_bytes / (kern_ms / 1e3) / 1e9
             traffic = None
-            tf = ROOT / "profiles" / "reply_level_traffic.json"
-            if tf.exists():
-                t = json.loads(tf.read_text())
-                if t.get("workload") == args.workload:
-                    traffic = t.get("dram_bytes_per_launch")
+            tf = ROOT / "profiles" / "reply_level_memory_bound.md"
+            if args.workload == "memory_bound" and not args.elements and tf.exists():
+                for line in tf.read_text().splitlines():
+                    if line.strip().startswith("traffic_bytes_per_launch"):
+                        traffic = int(line.split("=")[1])
             roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                         "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
                         "kernel": "reply_level_kernel", "peak_source": peaks["source"],
