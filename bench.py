@@ -242,6 +242,11 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
             dist.barrier()
 
     # ---- value: query resident in HBM -------------------------------------------------
+    # Workloads whose inputs fit in L2 (126 MB) get an L2 flush (a 512 MB write) before
+    # every step, outside the step's event pair; larger ones stream past L2 anyway.
+    input_bytes = db_bytes + nq * ct_words * 8
+    l2_flush = input_bytes < 2 * 126 * 2**20
+    flush_buf = torch.empty(512 * 2**20 // 8, dtype=torch.int64, device=f"cuda:{device}") if l2_flush else None
     for _ in range(args.warmup):
         ctx.reply(dbh, n, q_dev, out_dev)
     torch.cuda.synchronize()
@@ -254,6 +259,9 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
         t_end = torch.cuda.Event(enable_timing=True)
         t_start.record(stream)
         for k in range(args.steps):
+            if l2_flush:
+                with torch.cuda.stream(stream):
+                    flush_buf.fill_(k)
             evs[k][0].record(stream)
             ctx.reply(dbh, n, q_dev, out_dev)
             evs[k][1].record(stream)
@@ -261,8 +269,9 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
         torch.cuda.synchronize()
     barrier()
     launches = ctx.launch_count - launches0
-    elapsed_ms = t_start.elapsed_time(t_end)
     step_ms = [a.elapsed_time(b_) for a, b_ in evs]
+    # With flushes in the loop the timed work is the sum of the steps' own intervals.
+    elapsed_ms = sum(step_ms) if l2_flush else t_start.elapsed_time(t_end)
     clocks = clk.summary()
 
     # ---- e2e: host query in, host reply out, through the C ABI -------------------------
@@ -324,7 +333,8 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
             "config": {"workload": w["desc"], "N": N, "moduli": m, "d": len(n), "n": n, "alpha": alpha,
                        "elements": F, "element_bytes": L, "bits_per_coeff": b, "polys_per_element": P,
                        "imported_db_bytes": db_bytes, "query_bytes": query_bytes,
-                       "l2": "inputs larger than L2 (no flush needed)",
+                       "l2": ("L2 flushed before every step (512 MB write, outside the step timing)" if l2_flush
+                              else "inputs larger than L2 (no flush needed)"),
                        "parallelism": f"replicas{world}" if world > 1 else "single GPU"},
             "roofline": roofline,
             "cpu_baseline": cpu,

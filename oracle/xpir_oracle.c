@@ -407,6 +407,9 @@ int xo_reply_level(const uint64_t *db, uint64_t n_real, uint64_t P, uint64_t n_g
           uint64_t *rb = ra + mN;
           memset(ra, 0, KB * 8);
           memset(rb, 0, KB * 8);
+          /* A group made only of padding slots adds x = 0 terms (t = 0) to a zero start:
+           * its reply stays exactly zero. */
+          if ((uint64_t)j * n_i >= n_real) continue;
           for (uint64_t q = 0; q < n_i; q++) {
             const uint64_t e = (uint64_t)j * n_i + q;
             const uint64_t *ya = query + q * ct + c * N + k0, *yb = ya + mN;

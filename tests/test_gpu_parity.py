@@ -167,3 +167,20 @@ def test_context_close_releases_databases(engine, oracle):
     with engine.Context(1024, 1) as ctx2:
         d2 = ctx2.import_db(random_db(42, 10, 500), 10, 500, 1, oracle.bits_per_coeff(1024, 1, 10))
     del d2
+
+
+def test_full_size_recursive_config(engine, oracle):
+    """N=4096, 3 moduli, d=2 on a 1024x1024 grid, alpha=16, 1,048,576 elements x 256 B:
+    the full recursive configuration (65,536 aggregated elements, 983,040 zero-padding
+    slots never materialised), bit for bit against the oracle restatement."""
+    N, m, n, alpha, F, L = 4096, 3, [1024, 1024], 16, 1048576, 256
+    b, P = shapes(N, m, n, alpha, L, oracle)
+    assert (b, P) == (74, 1)
+    db = random_db(3, F, L)
+    q = random_query(5, n, N, m, oracle.moduli(m))
+    imp, rep = gpu_reply(engine, N, m, n, alpha, db, F, L, b, q)
+    want_imp = oracle.import_db(db, F, L, alpha, b, N, m)
+    assert np.array_equal(imp, want_imp)
+    want = oracle.reply(want_imp, F // alpha, P, n, q, b, N, m)
+    assert rep.size == want.size == 6 * 2 * m * N
+    assert np.array_equal(rep, want)
