@@ -120,6 +120,38 @@ XPIR_B200_API int xpir_b200_reply(xpir_b200_ctx *ctx, const xpir_b200_db *db, ui
                     int query_on_device, void *replies, uint64_t capacity_bytes, int out_on_device,
                     uint64_t *nb_replies);
 
+/* ---- batches of queries ---------------------------------------------------------- */
+/* One query of a batch.  Query and reply buffers are device memory. */
+typedef struct xpir_b200_request {
+  const xpir_b200_db *db;            /* imported database the query is for */
+  uint32_t d;                        /* PIRParameters.d */
+  uint32_t n[XPIR_B200_MAX_LEVELS];  /* PIRParameters.n */
+  const void *query;                 /* sum(n) ciphertexts, device memory */
+  void *replies;                     /* device memory for the final ciphertexts */
+  uint64_t capacity_bytes;
+  int status;                        /* out: XPIR_B200_* for this query */
+  uint64_t nb_replies;               /* out: reply ciphertexts written */
+} xpir_b200_request;
+
+/* Replies to `count` queries, possibly of different shapes and databases, in one
+ * submission: queries that share a database and a shape run as one launch per
+ * recursion level (the CTAs of all of them that read the same database tile run side
+ * by side and share it through L2), and the d > 1 queries' level replies are
+ * re-imported together.  Each reply is bit-identical to xpir_b200_reply's for the same
+ * query.  With use_graph != 0 the launches are captured in a CUDA graph, cached by the
+ * request list (databases, shapes and buffer addresses) and replayed when the same list
+ * is submitted again.  No counterpart in the reference, which answers one query per
+ * PIRReplyGenerator (pir/libpir.cpp:106-135); this is the batched form of that call.
+ * Returns XPIR_B200_OK if every query succeeded (see each request's status). */
+XPIR_B200_API int xpir_b200_reply_batch(xpir_b200_ctx *ctx, xpir_b200_request *reqs, uint32_t count, int use_graph);
+
+/* Times the compiled tile shapes of the reply kernel on this query's level shapes
+ * (queries in device memory; the replies are discarded) and keeps the fastest per
+ * shape for later xpir_b200_reply / xpir_b200_reply_batch calls on this context.
+ * *tile0 receives the choice for level 0.  No counterpart in the reference. */
+XPIR_B200_API int xpir_b200_autotune(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, const uint32_t *n,
+                                     const void *query_dev, int *tile0);
+
 /* ---- reply without allocation ---------------------------------------------------- */
 /* Bytes of device scratch available to xpir_b200_reply_noalloc (64 MiB). */
 #define XPIR_B200_NOALLOC_SCRATCH_BYTES (64ull << 20)

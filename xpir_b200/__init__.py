@@ -28,7 +28,16 @@ ERR_NODEV = -4
 ERR_STATE = -5
 ERR_TIMEOUT = -6
 
+MAX_LEVELS = 10
 _lib = None
+
+
+class Request(ctypes.Structure):
+    """xpir_b200_request: one query of a batch (device buffers)."""
+
+    _fields_ = [("db", ctypes.c_void_p), ("d", ctypes.c_uint32), ("n", ctypes.c_uint32 * MAX_LEVELS),
+                ("query", ctypes.c_void_p), ("replies", ctypes.c_void_p), ("capacity_bytes", ctypes.c_uint64),
+                ("status", ctypes.c_int), ("nb_replies", ctypes.c_uint64)]
 
 
 class XpirError(RuntimeError):
@@ -75,6 +84,8 @@ def _load():
         L.xpir_b200_db_export.argtypes = [vp, vp, c_u64]
         L.xpir_b200_reply.argtypes = [vp, vp, c_u32, ctypes.POINTER(c_u32), vp, ctypes.c_int, vp, c_u64,
                                       ctypes.c_int, ctypes.POINTER(c_u64)]
+        L.xpir_b200_reply_batch.argtypes = [vp, ctypes.POINTER(Request), c_u32, ctypes.c_int]
+        L.xpir_b200_autotune.argtypes = [vp, vp, c_u32, ctypes.POINTER(c_u32), vp, ctypes.POINTER(ctypes.c_int)]
         _lib = L
     return _lib
 
@@ -221,6 +232,31 @@ class Context:
                                        cap, _on_device(out), ctypes.byref(cnt)), "reply")
         assert cnt.value == Pl
         return out
+
+    def reply_batch(self, items, use_graph: bool = False) -> list[int]:
+        """Replies to several queries in one submission.  `items` are tuples
+        (database, n, query, replies) with query and replies in device memory (torch
+        CUDA tensors or raw device addresses).  Returns the per-query reply counts."""
+        reqs = (Request * len(items))()
+        for r, (db, n, q, out) in zip(reqs, items):
+            r.db = db.handle
+            r.d = len(n)
+            for j, v in enumerate(n):
+                r.n[j] = v
+            r.query = _ptr(q)
+            r.replies = _ptr(out)
+            r.capacity_bytes = out.numel() * out.element_size() if hasattr(out, "numel") else 2**63
+        status = _load().xpir_b200_reply_batch(self.handle, reqs, len(items), int(use_graph))
+        _check(status, "reply_batch")
+        return [r.nb_replies for r in reqs]
+
+    def autotune(self, db: Database, n: list[int], query) -> int:
+        """Times the compiled tile shapes on this query's shape and keeps the fastest."""
+        narr = (ctypes.c_uint32 * len(n))(*n)
+        tile = ctypes.c_int(-1)
+        _check(_load().xpir_b200_autotune(self.handle, db.handle, len(n), narr, _ptr(query), ctypes.byref(tile)),
+               "autotune")
+        return tile.value
 
     def close(self) -> None:
         if self.handle:

@@ -1,0 +1,349 @@
+// Batches of queries (xpir_b200_reply_batch), captured CUDA graphs of repeated batches,
+// and the tile-shape autotuner (xpir_b200_autotune).
+//
+// A batch is split into groups of queries that share a database and a shape (d, n).
+// Each group runs, per recursion level, one multi-task launch of the reply kernel (one
+// task per query: its own query and output, and at levels >= 1 its own re-imported
+// database), followed by one import launch that re-imports the level replies of all
+// the group's queries together.  The arithmetic per query is exactly xpir_b200_reply's.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "handles.h"
+#include "kernels.h"
+#include "params.h"
+#include "xpir_b200.h"
+
+using namespace xpir;
+
+namespace {
+
+int status_of(cudaError_t e) {
+  if (e == cudaSuccess) return XPIR_B200_OK;
+  (void)cudaGetLastError();
+  if (e == cudaErrorMemoryAllocation) return XPIR_B200_ERR_NOMEM;
+  if (e == cudaErrorNoDevice || e == cudaErrorInvalidDevice) return XPIR_B200_ERR_NODEV;
+  if (e == cudaErrorNotSupported) return XPIR_B200_ERR_ARG;
+  return XPIR_B200_ERR_CUDA;
+}
+
+struct Shape {
+  uint32_t d = 0;
+  uint64_t P[XPIR_B200_MAX_LEVELS] = {};
+  uint64_t groups[XPIR_B200_MAX_LEVELS] = {};
+  uint64_t n_real0 = 0;
+};
+
+// Level shapes of a query against `db` (the level loop of generateReply(),
+// pir/replyGenerator/PIRReplyGeneratorNFL_internal.cpp:366-429).  False if invalid.
+bool level_shapes(const xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, const uint32_t *n, Shape *sh) {
+  if (!db || db->ctx != ctx || d == 0 || d > XPIR_B200_MAX_LEVELS) return false;
+  uint64_t slots = 1;
+  for (uint32_t i = 0; i < d; i++) {
+    if (n[i] == 0 || slots > UINT64_MAX / n[i]) return false;
+    slots *= n[i];
+  }
+  if (slots < db->n_agg) return false;
+  const uint64_t ct_bits = 2ull * 64 * ctx->ps.m * ctx->ps.N;
+  sh->d = d;
+  sh->n_real0 = db->n_agg;
+  sh->P[0] = db->P;
+  for (uint32_t lvl = 0; lvl < d; lvl++) {
+    sh->groups[lvl] = 1;
+    for (uint32_t j = lvl + 1; j < d; j++) sh->groups[lvl] *= n[j];
+    if (lvl + 1 < d) sh->P[lvl + 1] = polys_for_bits(sh->P[lvl] * ct_bits, db->b, ctx->ps.N);
+  }
+  return true;
+}
+
+struct Group {
+  const xpir_b200_db *db;
+  uint32_t d;
+  uint32_t n[XPIR_B200_MAX_LEVELS];
+  Shape sh;
+  std::vector<uint32_t> reqs;
+};
+
+struct Sizes {
+  size_t ws_a = 0, ws_b = 0, tasks = 0;
+};
+
+Sizes sizes_of(const xpir_b200_ctx *ctx, const std::vector<Group> &groups) {
+  const uint64_t mN = (uint64_t)ctx->ps.m * ctx->ps.N, ct_bytes = 2 * mN * 8;
+  Sizes z;
+  for (const Group &g : groups) {
+    const uint64_t k = g.reqs.size();
+    z.tasks += k * g.d;
+    for (uint32_t lvl = 0; lvl + 1 < g.d; lvl++) {
+      z.ws_a = std::max<size_t>(z.ws_a, k * g.sh.groups[lvl] * g.sh.P[lvl] * ct_bytes);
+      z.ws_b = std::max<size_t>(z.ws_b, k * g.sh.groups[lvl] * g.sh.P[lvl + 1] * mN * 8);
+    }
+  }
+  return z;
+}
+
+// Enqueues every launch of the batch on the context's stream.
+cudaError_t enqueue(xpir_b200_ctx *ctx, const std::vector<Group> &groups, const xpir_b200_request *reqs,
+                    uint64_t *ws_a, uint64_t *ws_b, ReplyTask *host_tasks, ReplyTask *dev_tasks) {
+  const uint64_t mN = (uint64_t)ctx->ps.m * ctx->ps.N, ct_words = 2 * mN, ct_bytes = ct_words * 8;
+  size_t task_off = 0;
+  for (const Group &g : groups) {
+    ParamSet ps = ctx->ps;
+    ps.b = g.db->b;
+    const DevModuli dm = make_dev_moduli(ps);
+    const uint32_t k = (uint32_t)g.reqs.size();
+    std::vector<const uint64_t *> db(k), q(k);
+    std::vector<uint64_t *> out(k);
+    uint64_t q_off = 0;
+    for (uint32_t lvl = 0; lvl < g.d; lvl++) {
+      const bool last = lvl + 1 == g.d;
+      const uint64_t P = g.sh.P[lvl], groups_l = g.sh.groups[lvl];
+      const uint64_t n_real = lvl == 0 ? g.sh.n_real0 : g.sh.groups[lvl - 1];
+      for (uint32_t i = 0; i < k; i++) {
+        const xpir_b200_request &r = reqs[g.reqs[i]];
+        db[i] = lvl == 0 ? g.db->d_polys : ws_b + (uint64_t)i * n_real * P * mN;
+        q[i] = (const uint64_t *)r.query + q_off;
+        out[i] = last ? (uint64_t *)r.replies : ws_a + (uint64_t)i * groups_l * P * ct_words;
+      }
+      uint32_t launched = 0;
+      cudaError_t e = launch_reply_tasks(db.data(), q.data(), out.data(), k, n_real, P, groups_l, g.n[lvl], ps, dm,
+                                         host_tasks + task_off, dev_tasks + task_off, ctx->stream, &launched,
+                                         ctx->status_dev, tuned_tile(ctx, P, g.n[lvl], groups_l));
+      ctx->launches += launched;
+      if (e != cudaSuccess) return e;
+      task_off += k;
+      q_off += (uint64_t)g.n[lvl] * ct_words;
+      if (last) break;
+      // All queries' level replies are one run of k*groups elements of P ciphertexts.
+      const AggSource as{(const uint8_t *)ws_a, (uint64_t)k * groups_l, P * ct_bytes, P * ct_bytes, 1};
+      e = launch_import(as, (uint64_t)k * groups_l, g.sh.P[lvl + 1], ps, dm, ctx->d_tables, ws_b, ctx->stream);
+      ctx->launches++;
+      if (e != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
+}
+
+}  // namespace
+
+// A captured batch: its own workspaces and task tables, so that the graph stays valid
+// whatever else the context does.
+struct BatchPlan {
+  std::vector<uint64_t> key;
+  void *ws_a = nullptr, *ws_b = nullptr, *dev_tasks = nullptr, *host_tasks = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  ~BatchPlan() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaFree(ws_a);
+    cudaFree(ws_b);
+    cudaFree(dev_tasks);
+    if (host_tasks) cudaFreeHost(host_tasks);
+  }
+};
+
+namespace {
+
+std::vector<uint64_t> plan_key(const xpir_b200_ctx *ctx, const xpir_b200_request *reqs, uint32_t count,
+                               uint64_t tune_epoch) {
+  std::vector<uint64_t> key{tune_epoch, (uint64_t)(uintptr_t)ctx, count};
+  for (uint32_t i = 0; i < count; i++) {
+    key.push_back((uint64_t)(uintptr_t)reqs[i].db);
+    key.push_back(reqs[i].d);
+    for (uint32_t j = 0; j < reqs[i].d && j < XPIR_B200_MAX_LEVELS; j++) key.push_back(reqs[i].n[j]);
+    key.push_back((uint64_t)(uintptr_t)reqs[i].query);
+    key.push_back((uint64_t)(uintptr_t)reqs[i].replies);
+  }
+  return key;
+}
+
+constexpr size_t kMaxPlans = 8;
+
+}  // namespace
+
+extern "C" int xpir_b200_reply_batch(xpir_b200_ctx *ctx, xpir_b200_request *reqs, uint32_t count, int use_graph) {
+  if (!ctx || (!reqs && count)) return XPIR_B200_ERR_ARG;
+  if (count == 0) return XPIR_B200_OK;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return status_of(e);
+
+  // Validate and group.
+  const uint64_t ct_bytes = 2ull * ctx->ps.m * ctx->ps.N * 8;
+  std::vector<Group> groups;
+  int overall = XPIR_B200_OK;
+  for (uint32_t i = 0; i < count; i++) {
+    xpir_b200_request &r = reqs[i];
+    r.nb_replies = 0;
+    Shape sh;
+    if (!r.query || !r.replies || !level_shapes(ctx, r.db, r.d, r.n, &sh) ||
+        r.capacity_bytes < sh.P[sh.d - 1] * ct_bytes) {
+      r.status = XPIR_B200_ERR_ARG;
+      overall = XPIR_B200_ERR_ARG;
+      continue;
+    }
+    r.status = XPIR_B200_OK;
+    auto it = std::find_if(groups.begin(), groups.end(), [&](const Group &g) {
+      return g.db == r.db && g.d == r.d && memcmp(g.n, r.n, r.d * sizeof(uint32_t)) == 0;
+    });
+    if (it == groups.end()) {
+      Group g;
+      g.db = r.db;
+      g.d = r.d;
+      memset(g.n, 0, sizeof(g.n));
+      memcpy(g.n, r.n, r.d * sizeof(uint32_t));
+      g.sh = sh;
+      groups.push_back(g);
+      it = groups.end() - 1;
+    }
+    it->reqs.push_back(i);
+  }
+  if (groups.empty()) return overall;
+  const Sizes z = sizes_of(ctx, groups);
+  *ctx->status_host = 0;
+
+  auto finish = [&](cudaError_t err) -> int {
+    if (err == cudaSuccess) err = cudaStreamSynchronize(ctx->stream);
+    int rc = status_of(err);
+    if (rc == XPIR_B200_OK && *(volatile int *)ctx->status_host != 0) rc = XPIR_B200_ERR_TIMEOUT;
+    for (const Group &g : groups)
+      for (uint32_t i : g.reqs) {
+        reqs[i].status = rc;
+        if (rc == XPIR_B200_OK) reqs[i].nb_replies = g.sh.P[g.d - 1];
+      }
+    return rc != XPIR_B200_OK ? rc : overall;
+  };
+
+  if (!use_graph) {
+    // Context workspaces, plus a task table sized for this submission.
+    void *dev_tasks = nullptr, *host_tasks = nullptr;
+    auto cleanup = [&]() {
+      cudaFree(dev_tasks);
+      if (host_tasks) cudaFreeHost(host_tasks);
+    };
+    if (z.ws_a > ctx->ws_a_bytes) {
+      cudaFree(ctx->ws_a);
+      ctx->ws_a = nullptr;
+      ctx->ws_a_bytes = 0;
+      if ((e = cudaMalloc(&ctx->ws_a, z.ws_a)) != cudaSuccess) return status_of(e);
+      ctx->ws_a_bytes = z.ws_a;
+    }
+    if (z.ws_b > ctx->ws_b_bytes) {
+      cudaFree(ctx->ws_b);
+      ctx->ws_b = nullptr;
+      ctx->ws_b_bytes = 0;
+      if ((e = cudaMalloc(&ctx->ws_b, z.ws_b)) != cudaSuccess) return status_of(e);
+      ctx->ws_b_bytes = z.ws_b;
+    }
+    e = cudaMalloc(&dev_tasks, z.tasks * sizeof(ReplyTask));
+    if (e == cudaSuccess) e = cudaMallocHost(&host_tasks, z.tasks * sizeof(ReplyTask));
+    if (e == cudaSuccess)
+      e = enqueue(ctx, groups, reqs, (uint64_t *)ctx->ws_a, (uint64_t *)ctx->ws_b, (ReplyTask *)host_tasks,
+                  (ReplyTask *)dev_tasks);
+    const int rc = finish(e);
+    cleanup();
+    return rc;
+  }
+
+  // Graph path: replay a captured plan for the same request list, or capture one.
+  const std::vector<uint64_t> key = plan_key(ctx, reqs, count, ctx->tune_epoch);
+  for (auto &pl : ctx->plans)
+    if (pl->key == key) return finish(cudaGraphLaunch(pl->exec, ctx->stream));
+  auto plan = std::make_shared<BatchPlan>();
+  plan->key = key;
+  e = cudaMalloc(&plan->ws_a, std::max<size_t>(z.ws_a, 256));
+  if (e == cudaSuccess) e = cudaMalloc(&plan->ws_b, std::max<size_t>(z.ws_b, 256));
+  if (e == cudaSuccess) e = cudaMalloc(&plan->dev_tasks, z.tasks * sizeof(ReplyTask));
+  if (e == cudaSuccess) e = cudaMallocHost(&plan->host_tasks, z.tasks * sizeof(ReplyTask));
+  // One eager run first: it sets the kernels' attributes outside the capture and
+  // produces this submission's replies.
+  if (e == cudaSuccess)
+    e = enqueue(ctx, groups, reqs, (uint64_t *)plan->ws_a, (uint64_t *)plan->ws_b, (ReplyTask *)plan->host_tasks,
+                (ReplyTask *)plan->dev_tasks);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    const cudaError_t ee = enqueue(ctx, groups, reqs, (uint64_t *)plan->ws_a, (uint64_t *)plan->ws_b,
+                                   (ReplyTask *)plan->host_tasks, (ReplyTask *)plan->dev_tasks);
+    e = cudaStreamEndCapture(ctx->stream, &plan->graph);
+    if (ee != cudaSuccess) e = ee;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&plan->exec, plan->graph, 0);
+  if (e != cudaSuccess) return finish(e);
+  if (ctx->plans.size() >= kMaxPlans) ctx->plans.erase(ctx->plans.begin());
+  ctx->plans.push_back(plan);
+  return finish(cudaSuccess);
+}
+
+extern "C" int xpir_b200_autotune(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, const uint32_t *n,
+                                  const void *query_dev, int *tile0) {
+  if (!ctx || !n || !query_dev) return XPIR_B200_ERR_ARG;
+  Shape sh;
+  if (!level_shapes(ctx, db, d, n, &sh)) return XPIR_B200_ERR_ARG;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return status_of(e);
+  ParamSet ps = ctx->ps;
+  ps.b = db->b;
+  const DevModuli dm = make_dev_moduli(ps);
+  const uint64_t mN = (uint64_t)ps.m * ps.N, ct_words = 2 * mN, ct_bytes = ct_words * 8;
+  size_t rep_max = 0, next_max = 0;
+  for (uint32_t lvl = 0; lvl < d; lvl++) {
+    rep_max = std::max<size_t>(rep_max, sh.groups[lvl] * sh.P[lvl] * ct_bytes);
+    if (lvl + 1 < d) next_max = std::max<size_t>(next_max, sh.groups[lvl] * sh.P[lvl + 1] * mN * 8);
+  }
+  uint64_t *rep = nullptr, *next = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  e = cudaMalloc(&rep, rep_max);
+  if (e == cudaSuccess && next_max) e = cudaMalloc(&next, next_max);
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  *ctx->status_host = 0;
+  const uint64_t *in = db->d_polys;
+  const uint64_t *q = (const uint64_t *)query_dev;
+  uint64_t in_real = db->n_agg;
+  for (uint32_t lvl = 0; lvl < d && e == cudaSuccess; lvl++) {
+    ReplyLevelArgs a{in, in_real, sh.P[lvl], sh.groups[lvl], n[lvl], q, rep};
+    int best = -1;
+    float best_ms = 0;
+    for (int cand : tile_candidates(sh.P[lvl])) {
+      float ms = 0;
+      for (int rep_i = 0; rep_i < 2 && e == cudaSuccess; rep_i++) {  // the first run warms up
+        e = cudaEventRecord(e0, ctx->stream);
+        if (e == cudaSuccess) e = launch_reply_level(a, ps, dm, ctx->stream, nullptr, ctx->status_dev, cand);
+        if (e == cudaSuccess) e = cudaEventRecord(e1, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      }
+      if (e != cudaSuccess) break;
+      if (best < 0 || ms < best_ms) {
+        best = cand;
+        best_ms = ms;
+      }
+    }
+    if (e != cudaSuccess) break;
+    ctx->tuned[std::make_tuple(sh.P[lvl], (uint64_t)n[lvl], sh.groups[lvl])] = best;
+    if (lvl == 0 && tile0) *tile0 = best;
+    q += (uint64_t)n[lvl] * ct_words;
+    if (lvl + 1 == d) break;
+    const AggSource as{(const uint8_t *)rep, sh.groups[lvl], sh.P[lvl] * ct_bytes, sh.P[lvl] * ct_bytes, 1};
+    e = launch_import(as, sh.groups[lvl], sh.P[lvl + 1], ps, dm, ctx->d_tables, next, ctx->stream);
+    in = next;
+    in_real = sh.groups[lvl];
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  ctx->tune_epoch++;
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(rep);
+  cudaFree(next);
+  if (e == cudaSuccess && *(volatile int *)ctx->status_host != 0) return XPIR_B200_ERR_TIMEOUT;
+  return status_of(e);
+}

@@ -162,6 +162,7 @@ int xpir_b200_ctx_destroy(xpir_b200_ctx *ctx) {
   cudaFree(ctx->ws_query);
   cudaFree(ctx->ws_a);
   cudaFree(ctx->ws_b);
+  ctx->plans.clear();
   if (ctx->status_host) cudaFreeHost(ctx->status_host);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -334,7 +335,8 @@ int xpir_b200_reply(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, cons
     uint64_t *rep = (last && out_on_device) ? (uint64_t *)replies : (uint64_t *)ctx->ws_a;
     uint32_t launched = 0;
     ReplyLevelArgs a{in, in_real, Ps[lvl], groups[lvl], n[lvl], dq, rep};
-    const cudaError_t le = launch_reply_level(a, ps, dm, ctx->stream, &launched, ctx->status_dev);
+    const cudaError_t le = launch_reply_level(a, ps, dm, ctx->stream, &launched, ctx->status_dev,
+                                              tuned_tile(ctx, Ps[lvl], n[lvl], groups[lvl]));
     if (le == cudaErrorNotSupported) return XPIR_B200_ERR_ARG;
     XPIR_TRY(le);
     ctx->launches += launched;

@@ -4,12 +4,20 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
+#include <memory>
 #include <mutex>
 #include <set>
+#include <tuple>
+#include <vector>
 
 #include "params.h"
 
 struct xpir_b200_db;
+struct BatchPlan;  // batch.cu
+
+// Tile-shape choices made by xpir_b200_autotune, keyed by level shape (P, n_i, groups).
+typedef std::map<std::tuple<uint64_t, uint64_t, uint64_t>, int> TuneTable;
 
 struct xpir_b200_ctx {
   int device = 0;
@@ -28,7 +36,16 @@ struct xpir_b200_ctx {
   int *status_host = nullptr;  // kernel status word (mapped pinned memory)
   int *status_dev = nullptr;
   std::set<xpir_b200_db *> dbs;  // databases imported through this context
+  TuneTable tuned;
+  uint64_t tune_epoch = 0;  // bumped by every autotune (invalidates captured batches)
+  std::vector<std::shared_ptr<BatchPlan>> plans;  // captured batches (batch.cu)
 };
+
+// Tile shape for a level shape: the autotuned one if any, else -1 (default).
+inline int tuned_tile(const xpir_b200_ctx *ctx, uint64_t P, uint64_t n_i, uint64_t groups) {
+  auto it = ctx->tuned.find(std::make_tuple(P, n_i, groups));
+  return it == ctx->tuned.end() ? -1 : it->second;
+}
 
 struct xpir_b200_db {
   xpir_b200_ctx *ctx = nullptr;

@@ -1,8 +1,11 @@
 // Kernel launchers of the B200 reply engine (device code in import.cu / reply.cu).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <vector>
 
 #include "params.h"
 
@@ -55,7 +58,37 @@ struct ReplyLevelArgs {
 // `status` is a device-visible int that a kernel sets to a nonzero KernelStatus when one
 // of its bounded waits gives up (sm100.cuh); the caller clears and reads it.
 cudaError_t launch_reply_level(const ReplyLevelArgs &a, const ParamSet &ps, const DevModuli &dm,
-                               cudaStream_t stream, uint32_t *launches, int *status);
+                               cudaStream_t stream, uint32_t *launches, int *status, int tile = -1);
+
+// One task of a multi-task reply-level launch: the DB level of the task viewed as
+// [element][poly][modulus][coefficient], its query level as [slot][half][modulus][coefficient],
+// and its output [group][poly][half][modulus][coefficient].  Built on the host, copied
+// to device memory, read by the kernel (TMA takes the tensor maps' global addresses).
+struct alignas(128) ReplyTask {
+  CUtensorMap tm_db;
+  CUtensorMap tm_q;
+  uint64_t *out;
+};
+
+// A compiled tile shape of the reply kernel: W coefficients per slice, C poly columns
+// per CTA, E slots per tile, NS pipeline stages, TB term buffers.
+struct TileShape {
+  int W, C, E, NS, TB;
+};
+// Index of the default shape for a level with P polys per element.
+int default_tile(uint64_t P);
+// Shapes the autotuner may try for a level with P polys per element.
+std::vector<int> tile_candidates(uint64_t P);
+TileShape tile_shape(int tile);
+int tile_count();
+
+// `ntasks` reply levels of the same shape (n_real, P, n_groups, n_i), one per query,
+// in one launch.  `host_tasks` (pinned, ntasks entries) is filled here and copied to
+// `dev_tasks` on `stream` before the launch.  tile < 0 picks the default shape.
+cudaError_t launch_reply_tasks(const uint64_t *const *db, const uint64_t *const *query, uint64_t *const *out,
+                               uint32_t ntasks, uint64_t n_real, uint64_t P, uint64_t n_groups, uint64_t n_i,
+                               const ParamSet &ps, const DevModuli &dm, ReplyTask *host_tasks, ReplyTask *dev_tasks,
+                               cudaStream_t stream, uint32_t *launches, int *status, int tile);
 
 // Whether the reply kernel supports this level shape (moduli with the fast Shoup-factor
 // path, degree a multiple of the slice width, 32-bit TMA coordinates).

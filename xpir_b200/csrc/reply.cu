@@ -80,10 +80,12 @@ struct LevelShape {
 };
 
 
+// The work of one CTA: group g, coefficient slice blockIdx.y, modulus / column block
+// blockIdx.z, with the DB and query tensor maps and the output of its task.
 template <int W, int C, int E, int NS, int TB>
-__global__ void __launch_bounds__(Cfg<W, C, E, NS, TB>::kThreads, C <= 2 ? 2 : 1)
-    reply_tma_kernel(const __grid_constant__ CUtensorMap tm_db, const __grid_constant__ CUtensorMap tm_q,
-                     uint64_t *__restrict__ out, const LevelShape sh, const DevModuli dm, int *status) {
+__device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUtensorMap *tm_q,
+                                           uint64_t *__restrict__ out, const uint64_t g, const LevelShape &sh,
+                                           const DevModuli &dm, int *status) {
   using S = Cfg<W, C, E, NS, TB>;
   constexpr int kComputeWarps = S::kComputeWarps;
   constexpr int kComputeThreads = S::kComputeThreads;
@@ -96,7 +98,6 @@ __global__ void __launch_bounds__(Cfg<W, C, E, NS, TB>::kThreads, C <= 2 ? 2 : 1
   uint64_t *full = bars, *empty = bars + NS, *tfull = bars + 2 * NS, *tempty = bars + 2 * NS + TB;
 
   const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const uint64_t g = blockIdx.x;
   const int k0 = blockIdx.y * kW;
   const uint32_t c = blockIdx.z / sh.col_blocks;
   const uint32_t cp0 = (blockIdx.z - c * sh.col_blocks) * C;
@@ -123,8 +124,8 @@ __global__ void __launch_bounds__(Cfg<W, C, E, NS, TB>::kThreads, C <= 2 ? 2 : 1
   if (warp == 0) {
     // ---- TMA producer ------------------------------------------------------------
     if (lane == 0) {
-      tma_prefetch_desc(&tm_db);
-      tma_prefetch_desc(&tm_q);
+      tma_prefetch_desc(tm_db);
+      tma_prefetch_desc(tm_q);
       constexpr uint32_t kTx = (uint32_t)((S::kX + S::kQ) * 8);
       uint32_t t = 0;
       for (; t < tiles; ++t) {
@@ -135,8 +136,8 @@ __global__ void __launch_bounds__(Cfg<W, C, E, NS, TB>::kThreads, C <= 2 ? 2 : 1
         }
         mbar_arrive_expect_tx(full + s, kTx);
         const int slot = (int)t * E;
-        tma_load_4d(xs + s * S::kX, &tm_db, k0, (int)c, (int)cp0, (int)(g * sh.n_i) + slot, full + s);
-        tma_load_4d(qs + s * S::kQ, &tm_q, k0, (int)c, 0, slot, full + s);
+        tma_load_4d(xs + s * S::kX, tm_db, k0, (int)c, (int)cp0, (int)(g * sh.n_i) + slot, full + s);
+        tma_load_4d(qs + s * S::kQ, tm_q, k0, (int)c, 0, slot, full + s);
       }
       // Drain: every issued copy must have landed before the CTA exits.
       const uint32_t first = t > (uint32_t)NS ? t - NS : 0;
@@ -230,32 +231,111 @@ __global__ void __launch_bounds__(Cfg<W, C, E, NS, TB>::kThreads, C <= 2 ? 2 : 1
   }
 }
 
-template <int W, int C, int E, int NS, int TB = 2>
-cudaError_t launch_c(const ReplyLevelArgs &a, const ParamSet &ps, const DevModuli &dm, uint64_t groups,
-                     cudaStream_t stream, int *status) {
-  // DB level viewed as [element][poly][modulus][coefficient]; query as [slot][half][modulus][coefficient].
+// One query: tensor maps as grid constants.  Grid: x = group.
+template <int W, int C, int E, int NS, int TB>
+__global__ void __launch_bounds__(Cfg<W, C, E, NS, TB>::kThreads, C <= 2 ? 2 : 1)
+    reply_tma_kernel(const __grid_constant__ CUtensorMap tm_db, const __grid_constant__ CUtensorMap tm_q,
+                     uint64_t *__restrict__ out, const LevelShape sh, const DevModuli dm, int *status) {
+  reply_tile<W, C, E, NS, TB>(&tm_db, &tm_q, out, blockIdx.x, sh, dm, status);
+}
+
+// Several tasks of one level shape (a batch of queries): each task's tensor maps and
+// output come from a descriptor table in global memory.  Grid: x = group * tasks + task,
+// so the CTAs of all queries that read the same DB tile run side by side and share it
+// through L2.
+template <int W, int C, int E, int NS, int TB>
+__global__ void __launch_bounds__(Cfg<W, C, E, NS, TB>::kThreads, C <= 2 ? 2 : 1)
+    reply_tma_tasks_kernel(const ReplyTask *__restrict__ tasks, const uint32_t ntasks, const LevelShape sh,
+                           const DevModuli dm, int *status) {
+  const uint32_t t = blockIdx.x % ntasks;
+  reply_tile<W, C, E, NS, TB>(&tasks[t].tm_db, &tasks[t].tm_q, tasks[t].out, blockIdx.x / ntasks, sh, dm, status);
+}
+
+// Tensor maps of one task for tile shape (W, C, E).
+template <int W, int C, int E>
+bool encode_task(const uint64_t *db, const uint64_t *query, uint64_t n_real, uint64_t P, uint64_t n_i,
+                 const ParamSet &ps, CUtensorMap *tm_db, CUtensorMap *tm_q) {
   const uint64_t N = ps.N, m = ps.m;
-  CUtensorMap tm_db, tm_q;
-  const uint64_t db_dims[4] = {N, m, a.P, a.n_real};
-  const uint64_t db_strides[3] = {N * 8, m * N * 8, a.P * m * N * 8};
+  const uint64_t db_dims[4] = {N, m, P, n_real};
+  const uint64_t db_strides[3] = {N * 8, m * N * 8, P * m * N * 8};
   const uint32_t db_box[4] = {(uint32_t)W, 1, (uint32_t)C, (uint32_t)E};
-  const uint64_t q_dims[4] = {N, m, 2, a.n_i};
+  const uint64_t q_dims[4] = {N, m, 2, n_i};
   const uint64_t q_strides[3] = {N * 8, m * N * 8, 2 * m * N * 8};
   const uint32_t q_box[4] = {(uint32_t)W, 1, 2, (uint32_t)E};
-  if (!encode_tensor_map_u64_4d(&tm_db, a.db, db_dims, db_strides, db_box) ||
-      !encode_tensor_map_u64_4d(&tm_q, a.query, q_dims, q_strides, q_box))
-    return cudaErrorInvalidValue;
+  return encode_tensor_map_u64_4d(tm_db, db, db_dims, db_strides, db_box) &&
+         encode_tensor_map_u64_4d(tm_q, query, q_dims, q_strides, q_box);
+}
+
+template <int W, int C, int E, int NS, int TB>
+cudaError_t launch_c(const ReplyLevelArgs &a, const ParamSet &ps, const DevModuli &dm, uint64_t groups,
+                     cudaStream_t stream, int *status) {
+  CUtensorMap tm_db, tm_q;
+  if (!encode_task<W, C, E>(a.db, a.query, a.n_real, a.P, a.n_i, ps, &tm_db, &tm_q)) return cudaErrorInvalidValue;
   using S = Cfg<W, C, E, NS, TB>;
   auto kern = reply_tma_kernel<W, C, E, NS, TB>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kBytes);
   if (e != cudaSuccess) return e;
   const uint32_t col_blocks = (uint32_t)((a.P + C - 1) / C);
   LevelShape sh{a.n_real, a.P, a.n_i, ps.N, ps.m, col_blocks};
-  if (groups > 0x7fffffffull || (uint64_t)m * col_blocks > 65535) return cudaErrorInvalidValue;
-  dim3 grid((unsigned)groups, ps.N / W, (unsigned)(m * col_blocks));
+  if (groups > 0x7fffffffull || (uint64_t)ps.m * col_blocks > 65535) return cudaErrorInvalidValue;
+  dim3 grid((unsigned)groups, ps.N / W, (unsigned)(ps.m * col_blocks));
   kern<<<grid, S::kThreads, S::kBytes, stream>>>(tm_db, tm_q, a.out, sh, dm, status);
   return cudaGetLastError();
 }
+
+template <int W, int C, int E, int NS, int TB>
+cudaError_t launch_tasks_c(const uint64_t *const *db, const uint64_t *const *query, uint64_t *const *out,
+                           uint32_t ntasks, uint64_t n_real, uint64_t P, uint64_t groups, uint64_t n_i,
+                           const ParamSet &ps, const DevModuli &dm, ReplyTask *host_tasks, ReplyTask *dev_tasks,
+                           cudaStream_t stream, int *status) {
+  for (uint32_t t = 0; t < ntasks; t++) {
+    if (!encode_task<W, C, E>(db[t], query[t], n_real, P, n_i, ps, &host_tasks[t].tm_db, &host_tasks[t].tm_q))
+      return cudaErrorInvalidValue;
+    host_tasks[t].out = out[t];
+  }
+  cudaError_t e = cudaMemcpyAsync(dev_tasks, host_tasks, ntasks * sizeof(ReplyTask), cudaMemcpyHostToDevice, stream);
+  if (e != cudaSuccess) return e;
+  using S = Cfg<W, C, E, NS, TB>;
+  auto kern = reply_tma_tasks_kernel<W, C, E, NS, TB>;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kBytes);
+  if (e != cudaSuccess) return e;
+  const uint32_t col_blocks = (uint32_t)((P + C - 1) / C);
+  LevelShape sh{n_real, P, n_i, ps.N, ps.m, col_blocks};
+  if (groups * ntasks > 0x7fffffffull || (uint64_t)ps.m * col_blocks > 65535) return cudaErrorInvalidValue;
+  dim3 grid((unsigned)(groups * ntasks), ps.N / W, (unsigned)(ps.m * col_blocks));
+  kern<<<grid, S::kThreads, S::kBytes, stream>>>(dev_tasks, ntasks, sh, dm, status);
+  return cudaGetLastError();
+}
+
+typedef cudaError_t (*SingleFn)(const ReplyLevelArgs &, const ParamSet &, const DevModuli &, uint64_t, cudaStream_t,
+                                int *);
+typedef cudaError_t (*TasksFn)(const uint64_t *const *, const uint64_t *const *, uint64_t *const *, uint32_t, uint64_t,
+                               uint64_t, uint64_t, uint64_t, const ParamSet &, const DevModuli &, ReplyTask *,
+                               ReplyTask *, cudaStream_t, int *);
+struct TileEntry {
+  TileShape shape;
+  SingleFn single;
+  TasksFn tasks;
+};
+
+#define XPIR_TILE(W, C, E, NS, TB) \
+  { {W, C, E, NS, TB}, &launch_c<W, C, E, NS, TB>, &launch_tasks_c<W, C, E, NS, TB> }
+
+// Every compiled tile shape.  Entry 0..2: one poly column (the defaults and the
+// autotuner's alternatives for P = 1); then one entry per column count 2..8.
+const TileEntry kTiles[] = {
+    XPIR_TILE(XPIR_P1_W, 1, XPIR_P1_E, XPIR_P1_NS, XPIR_P1_TB),
+    XPIR_TILE(16, 1, 32, 4, 4),
+    XPIR_TILE(32, 1, 32, 3, 4),
+    XPIR_TILE(16, 2, 32, 3, 2),
+    XPIR_TILE(16, 3, 16, 4, 2),
+    XPIR_TILE(16, 4, 16, 3, 2),
+    XPIR_TILE(16, 5, 16, 3, 2),
+    XPIR_TILE(16, 6, 16, 3, 2),
+    XPIR_TILE(16, 7, 16, 3, 2),
+    XPIR_TILE(16, 8, 16, 3, 2),
+};
+constexpr int kTileCount = sizeof(kTiles) / sizeof(kTiles[0]);
 
 }  // namespace
 
@@ -266,8 +346,42 @@ bool reply_level_supported(const ParamSet &ps, uint64_t n_real, uint64_t n_i, ui
   return ps.N % 16 == 0 && n_real < (1ull << 31) && groups * n_i + 256 < (1ull << 31);
 }
 
+int default_tile(uint64_t P) { return P <= 1 ? 0 : (int)(P >= 8 ? 9 : P + 1); }
+
+std::vector<int> tile_candidates(uint64_t P) {
+  if (P <= 1) return {0, 1, 2};
+  // several columns per CTA (query factors shared) or one column per CTA
+  return {default_tile(P), 0};
+}
+
+TileShape tile_shape(int tile) { return kTiles[tile].shape; }
+int tile_count() { return kTileCount; }
+
+cudaError_t launch_reply_tasks(const uint64_t *const *db, const uint64_t *const *query, uint64_t *const *out,
+                               uint32_t ntasks, uint64_t n_real, uint64_t P, uint64_t n_groups, uint64_t n_i,
+                               const ParamSet &ps, const DevModuli &dm, ReplyTask *host_tasks, ReplyTask *dev_tasks,
+                               cudaStream_t stream, uint32_t *launches, int *status, int tile) {
+  if (ntasks == 0) return cudaSuccess;
+  const uint64_t ct_words = 2ull * ps.m * ps.N;
+  uint64_t active = n_i == 0 ? 0 : (n_real + n_i - 1) / n_i;
+  if (active > n_groups) active = n_groups;
+  if (active < n_groups) {
+    for (uint32_t t = 0; t < ntasks; t++) {
+      cudaError_t e = cudaMemsetAsync(out[t] + active * P * ct_words, 0,
+                                      (n_groups - active) * P * ct_words * sizeof(uint64_t), stream);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  if (active == 0) return cudaSuccess;
+  if (!reply_level_supported(ps, n_real, n_i, active * ntasks)) return cudaErrorNotSupported;
+  if (tile < 0 || tile >= kTileCount || kTiles[tile].shape.C > (int)(P > 8 ? 8 : P)) tile = default_tile(P);
+  if (launches) (*launches)++;
+  return kTiles[tile].tasks(db, query, out, ntasks, n_real, P, active, n_i, ps, dm, host_tasks, dev_tasks, stream,
+                            status);
+}
+
 cudaError_t launch_reply_level(const ReplyLevelArgs &a, const ParamSet &ps, const DevModuli &dm,
-                               cudaStream_t stream, uint32_t *launches, int *status) {
+                               cudaStream_t stream, uint32_t *launches, int *status, int tile) {
   const uint64_t ct_words = 2ull * ps.m * ps.N;
   // Groups whose every slot is past the real elements accumulate only zero terms from
   // a zero start: their replies are exactly zero.  Only groups with data are launched.
@@ -281,17 +395,8 @@ cudaError_t launch_reply_level(const ReplyLevelArgs &a, const ParamSet &ps, cons
   if (active == 0) return cudaSuccess;
   if (!reply_level_supported(ps, a.n_real, a.n_i, active)) return cudaErrorNotSupported;
   if (launches) (*launches)++;
-  // Tile shapes per poly-column count (W, C, E, NS[, term buffers]).
-  switch (a.P) {
-    case 1: return launch_c<XPIR_P1_W, 1, XPIR_P1_E, XPIR_P1_NS, XPIR_P1_TB>(a, ps, dm, active, stream, status);
-    case 2: return launch_c<16, 2, 32, 3>(a, ps, dm, active, stream, status);
-    case 3: return launch_c<16, 3, 16, 4>(a, ps, dm, active, stream, status);
-    case 4: return launch_c<16, 4, 16, 3>(a, ps, dm, active, stream, status);
-    case 5: return launch_c<16, 5, 16, 3>(a, ps, dm, active, stream, status);
-    case 6: return launch_c<16, 6, 16, 3>(a, ps, dm, active, stream, status);
-    case 7: return launch_c<16, 7, 16, 3>(a, ps, dm, active, stream, status);
-    default: return launch_c<16, 8, 16, 3>(a, ps, dm, active, stream, status);
-  }
+  if (tile < 0 || tile >= kTileCount || kTiles[tile].shape.C > (int)(a.P > 8 ? 8 : a.P)) tile = default_tile(a.P);
+  return kTiles[tile].single(a, ps, dm, active, stream, status);
 }
 
 }  // namespace xpir
