@@ -136,6 +136,7 @@ cudaError_t enqueue(xpir_b200_ctx *ctx, const std::vector<Group> &groups, const 
 // whatever else the context does.
 struct BatchPlan {
   std::vector<uint64_t> key;
+  uint64_t launches = 0;  // engine kernels in the captured graph
   void *ws_a = nullptr, *ws_b = nullptr, *dev_tasks = nullptr, *host_tasks = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -255,7 +256,10 @@ extern "C" int xpir_b200_reply_batch(xpir_b200_ctx *ctx, xpir_b200_request *reqs
   // Graph path: replay a captured plan for the same request list, or capture one.
   const std::vector<uint64_t> key = plan_key(ctx, reqs, count, ctx->tune_epoch);
   for (auto &pl : ctx->plans)
-    if (pl->key == key) return finish(cudaGraphLaunch(pl->exec, ctx->stream));
+    if (pl->key == key) {
+      ctx->launches += pl->launches;
+      return finish(cudaGraphLaunch(pl->exec, ctx->stream));
+    }
   auto plan = std::make_shared<BatchPlan>();
   plan->key = key;
   e = cudaMalloc(&plan->ws_a, std::max<size_t>(z.ws_a, 256));
@@ -270,8 +274,11 @@ extern "C" int xpir_b200_reply_batch(xpir_b200_ctx *ctx, xpir_b200_request *reqs
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e == cudaSuccess) e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
+    const uint64_t before = ctx->launches;
     const cudaError_t ee = enqueue(ctx, groups, reqs, (uint64_t *)plan->ws_a, (uint64_t *)plan->ws_b,
                                    (ReplyTask *)plan->host_tasks, (ReplyTask *)plan->dev_tasks);
+    plan->launches = ctx->launches - before;
+    ctx->launches = before;  // captured, not launched
     e = cudaStreamEndCapture(ctx->stream, &plan->graph);
     if (ee != cudaSuccess) e = ee;
   }
