@@ -25,6 +25,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import sys
@@ -51,6 +52,20 @@ WORKLOADS = {
     "batched": dict(N=2048, m=2, F=65536, L=8192, sample=8192,
                     classes=[(32, [65536], 1), (16, [16384], 4), (16, [256, 256], 1)],
                     desc="batched: LWE:80:2048:120, 65536 x 8 KB, 64 queries (32 d1/a1, 16 d1/a4, 16 d2 256x256)"),
+    # Serving loop over three resident databases, one lane (context) each.  mix: (database,
+    # d, alpha, weight) of the admitted shapes; grids from the client optimizer's rule.
+    "serving": dict(dbs=[("DB1", 1024, 1, 200000, 2048), ("DB2", 2048, 2, 100000, 8192),
+                         ("DB3", 4096, 3, 1 << 20, 256)],
+                    mix=[(0, 2, 1, 20), (0, 2, 4, 20), (0, 2, 16, 20), (0, 1, 16, 4),
+                         (1, 2, 1, 20), (1, 2, 4, 20), (1, 2, 16, 20), (1, 1, 16, 4),
+                         (2, 2, 16, 20), (2, 2, 4, 8), (2, 1, 16, 1)],
+                    not_admitted="DB3 alpha=1 (103 GB imported; a d=1 query is 206 GB) and d=1 at alpha<16 "
+                                 "(3.3-51.5 GB queries): larger than the device budget or HBM",
+                    rates=[10, 100, 500, 2000], seconds=4.0, min_queries=40, max_queries=600,
+                    budget=40 << 30, max_batch=16, sample_div=20,
+                    desc="serving: DB1 LWE:80:1024:60 200000 x 2 KB, DB2 LWE:80:2048:120 100000 x 8 KB, "
+                         "DB3 LWE:80:4096:180 1048576 x 256 B; Poisson arrivals; mixed d in {1,2}, "
+                         "alpha in {1,4,16}"),
 }
 
 
@@ -514,6 +529,267 @@ def reference_batched_arm(args, w: dict, world: int, rank: int) -> int:
     print(json.dumps(line))
     return 0
 
+def dim_sizes(n: int, alpha: int, d: int) -> list[int]:
+    """Grid of a d-dimensional query over n elements aggregated by alpha: the client
+    optimizer's rule (apps/optim/PIROptimizer.cpp:338-365), d equal sides of
+    floor((n/alpha)^(1/d)), incremented one by one until their product covers n/alpha."""
+    new_n = -(-n // alpha)
+    f = [math.floor(new_n ** (1.0 / d))] * d
+    if f[0] != new_n ** (1.0 / d):
+        prod, j = 1, 0
+        while prod < new_n and j < d:
+            f[j] += 1
+            j += 1
+            prod = math.prod(f)
+    return f
+
+
+def serving_shapes(w: dict) -> list[dict]:
+    import xpir_b200
+
+    shapes = []
+    for k, (db, d, alpha, weight) in enumerate(w["mix"]):
+        name, N, m, F, L = w["dbs"][db]
+        n = dim_sizes(F, alpha, d)
+        b = xpir_b200.bits_per_coeff(N, m, n[0])
+        ct = xpir_b200.ciphertext_bytes(N, m)
+        shapes.append(dict(id=k, db=db, name=f"{name} d{d} a{alpha}", N=N, m=m, F=F, L=L, d=d, alpha=alpha, n=n,
+                           b=b, weight=weight, query_bytes=sum(n) * ct,
+                           reply_bytes=xpir_b200.reply_count(L, alpha, d, b, N, m) * ct))
+    return shapes
+
+
+def reference_mix(w: dict, threads: int) -> dict:
+    """The reference, one query at a time, on a 1/sample_div sample of every admitted
+    shape (the grid recomputed for the sample), each reply time scaled to the full
+    database; the mix's queries/s weights the shapes as the arrivals do."""
+    from oracle import pyoracle as po
+
+    if not po.ref_available():
+        return {"unavailable": "reference checker oracle/_ref/xpir_ref was not built"}
+    per, tot_w, tot_s = [], 0.0, 0.0
+    for sh in serving_shapes(w):
+        S = max(sh["alpha"] * 64, sh["F"] // w["sample_div"])
+        n = dim_sizes(S, sh["alpha"], sh["d"])
+        db = synthetic_db(11 + sh["db"], S, sh["L"])
+        r = po.ref_run(sh["N"], sh["m"], n, sh["alpha"], db, S, sh["L"], keyseed=2000 + sh["id"], chosen=0,
+                       extract=False, threads=threads)
+        full_s = r["reply_s"] * sh["F"] / S
+        per.append({"shape": sh["name"], "elements": S, "n": n, "reply_s": round(r["reply_s"], 4),
+                    "scaled_s": round(full_s, 3)})
+        tot_w += sh["weight"]
+        tot_s += sh["weight"] * full_s
+    return {"qps": tot_w / tot_s, "per_shape": per, "threads": threads}
+
+
+def serving_arm(args, w: dict, world: int, rank: int, local: int) -> int:
+    """Poisson arrivals of mixed queries through the serving loop (xpir_b200.Server): host
+    queries in, host replies out, admission by a device budget, continuous batching per
+    lane.  value = completed queries/s at the highest offered rate; every reply is checked
+    against the same query's reply computed alone."""
+    import queue
+    import threading
+
+    import torch
+
+    import xpir_b200
+
+    if world > 1 and rank != 0:
+        # Replicas only: every rank would run the same independent server; the serving
+        # measurement is taken on rank 0's GPU.
+        return 0
+    device = local
+    torch.cuda.set_device(device)
+    dev = f"cuda:{device}"
+    shapes = serving_shapes(w)
+    ctxs = [xpir_b200.Context(N, m, device=device) for (_, N, m, _, _) in w["dbs"]]
+    # Imports: one per (database, alpha, bits per coefficient), from device-resident bytes.
+    t0 = time.perf_counter()
+    imported = {}
+    for i, (name, N, m, F, L) in enumerate(w["dbs"]):
+        raw = torch.from_numpy(synthetic_db(11 + i, F, L)).to(dev)
+        for sh in shapes:
+            key = (i, sh["alpha"], sh["b"])
+            if sh["db"] == i and key not in imported:
+                imported[key] = ctxs[i].import_db(raw, F, L, sh["alpha"], sh["b"])
+        del raw
+    torch.cuda.synchronize()
+    import_s = time.perf_counter() - t0
+    resident = sum(d.device_bytes for d in imported.values())
+    log(f"imported {len(imported)} shapes, {resident / 1e9:.1f} GB resident, {import_s:.1f} s")
+    # Query pools (pinned host memory) and each query's reply computed alone.
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(5000)
+    pools, expect = {}, {}
+    for sh in shapes:
+        sh["dbh"] = imported[(sh["db"], sh["alpha"], sh["b"])]
+        k = max(1, min(3, int(1.5e9 // sh["query_bytes"])))
+        moduli = xpir_b200.moduli(sh["m"])
+        pools[sh["id"]] = []
+        for j in range(k):
+            q = torch.empty((sum(sh["n"]), 2, sh["m"], sh["N"]), dtype=torch.int64, device=dev)
+            for c in range(sh["m"]):  # uniform words mod p, the range of XPIR's query ciphertexts
+                q[:, :, c, :].random_(0, moduli[c], generator=gen)
+            qh = torch.empty(q.numel(), dtype=torch.int64, pin_memory=True)
+            qh.copy_(q.view(-1))
+            del q
+            pools[sh["id"]].append(qh)
+            expect[(sh["id"], j)] = ctxs[sh["db"]].reply(sh["dbh"], sh["n"], qh)
+        torch.cuda.synchronize()
+    log(f"query pools: {sum(q.numel() * 8 for v in pools.values() for q in v) / 1e9:.1f} GB pinned")
+    footprints = {sh["id"]: xpir_b200.Server.footprint(sh["dbh"], sh["n"]) for sh in shapes}
+    srv = xpir_b200.Server(ctxs, device_budget_bytes=w["budget"], max_batch=w["max_batch"])
+    weights = np.array([sh["weight"] for sh in shapes], dtype=np.float64)
+    weights /= weights.sum()
+
+    def run_rate(rate: float, count: int, seed: int) -> dict:
+        rng = np.random.default_rng(seed)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=count))
+        picks = rng.choice(len(shapes), size=count, p=weights)
+        which = [int(rng.integers(0, len(pools[int(s)]))) for s in picks]
+        rbytes = [shapes[int(s)]["reply_bytes"] for s in picks]
+        arena = torch.empty(sum(rbytes) // 8, dtype=torch.int64, pin_memory=True)
+        offs = np.concatenate([[0], np.cumsum(rbytes) // 8])
+        outs = [arena[offs[i]:offs[i + 1]] for i in range(count)]
+        pending: "queue.Queue" = queue.Queue()
+        sub_t = [0.0] * count
+        err: list = []
+
+        def submitter():
+            try:
+                start = time.perf_counter()
+                for i in range(count):
+                    delay = start + arrivals[i] - time.perf_counter()
+                    if delay > 0:
+                        time.sleep(delay)
+                    sh = shapes[int(picks[i])]
+                    sub_t[i] = time.perf_counter()
+                    pending.put((i, srv.submit(sh["dbh"], sh["n"], pools[sh["id"]][which[i]], outs[i])))
+            except Exception as e:
+                err.append(e)
+                pending.put(None)
+
+        l0 = sum(c.launch_count for c in ctxs)
+        st0 = srv.stats()
+        th = threading.Thread(target=submitter)
+        th.start()
+        lat, qd, done_t = [0.0] * count, [0.0] * count, [0.0] * count
+        for _ in range(count):
+            item = pending.get()
+            if item is None:
+                break
+            i, t = item
+            _, lat[i], qd[i] = srv.wait(t)
+            done_t[i] = sub_t[i] + lat[i]
+        th.join()
+        if err:
+            raise err[0]
+        st1 = srv.stats()
+        bad = sum(not np.array_equal(outs[i].numpy().view(np.uint64), expect[(int(picks[i]), which[i])])
+                  for i in range(count))
+        span = max(done_t) - min(sub_t)
+        lat_ms = np.array(lat) * 1e3
+        qbytes = sum(shapes[int(s)]["query_bytes"] for s in picks)
+        algo = sum(shapes[int(s)]["dbh"].device_bytes + shapes[int(s)]["query_bytes"] + shapes[int(s)]["reply_bytes"]
+                   for s in picks)
+        return {"offered_qps": rate, "queries": count, "achieved_qps": round(count / span, 2),
+                "p50_ms": round(float(np.percentile(lat_ms, 50)), 3),
+                "p99_ms": round(float(np.percentile(lat_ms, 99)), 3),
+                "queued_p50_ms": round(float(np.percentile(np.array(qd) * 1e3, 50)), 3),
+                "mean_batch": round((st1["completed"] - st0["completed"]) / max(1, st1["batches"] - st0["batches"]), 2),
+                "mismatches": int(bad), "span_s": round(span, 3), "launches": sum(c.launch_count for c in ctxs) - l0,
+                "h2d_bytes": qbytes, "d2h_bytes": sum(rbytes), "algorithmic_bytes": algo}
+
+    # Warm-up: every shape once per pool entry (pools, kernels, workspaces).
+    for _ in range(max(1, args.warmup)):
+        bufs = [(sh, j, np.empty(sh["reply_bytes"] // 8, dtype=np.uint64))
+                for sh in shapes for j in range(len(pools[sh["id"]]))]
+        ts = [srv.submit(sh["dbh"], sh["n"], pools[sh["id"]][j], out) for sh, j, out in bufs]
+        for t in ts:
+            srv.wait(t)
+        for sh, j, out in bufs:
+            if not np.array_equal(out, expect[(sh["id"], j)]):
+                raise RuntimeError(f"served reply of {sh['name']} differs from the reply computed alone")
+    results = []
+    with ClockSampler(device) as clk:
+        for k, rate in enumerate(w["rates"]):
+            count = int(min(w["max_queries"], max(w["min_queries"], rate * w["seconds"])))
+            results.append(run_rate(rate, count, 9000 + k))
+            log(f"rate {rate}: {results[-1]}")
+    clocks = clk.summary()
+    st = srv.stats()
+    srv.close()
+    mism = sum(r["mismatches"] for r in results)
+    top = results[-1]
+    peaks = measured_peaks()
+    achieved = top["algorithmic_bytes"] / top["span_s"] / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        r = reference_mix(w, os.cpu_count() or 1)
+        if "unavailable" not in r:
+            cpu = {"value": round(r["qps"], 4), "unit": "queries/s", "cores": r["threads"], "kind": "reference",
+                   "sample": f"one query per admitted shape on 1/{w['sample_div']} of its database, reply time "
+                             f"scaled to the full database, weighted as the arrivals",
+                   "per_shape": r["per_shape"]}
+    line = {
+        "metric": METRIC, "value": top["achieved_qps"], "unit": "queries/s", "n_gpus": 1, "steps": top["queries"],
+        "warmup": args.warmup, "ms_per_step": round(1e3 / top["achieved_qps"], 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic: seeded uniform DB bytes; query words uniform mod p, generated on the device and "
+                "held in pinned host memory",
+        "config": {"workload": w["desc"], "admitted_mix": [f"{sh['name']} n={sh['n']} w={sh['weight']}" for sh in shapes],
+                   "not_admitted": w["not_admitted"], "device_budget_bytes": w["budget"],
+                   "max_batch": w["max_batch"], "resident_db_bytes": resident, "import_s": round(import_s, 2),
+                   "lanes": len(ctxs), "footprints": {sh["name"]: footprints[sh["id"]] for sh in shapes},
+                   "l2": "inputs larger than L2 (no flush needed)", "parallelism": "single GPU"},
+        "rates": results,
+        "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"],
+        "bit_exact": mism == 0,
+        "server": st,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": None,
+                     "kernel": "whole serving run at the highest offered rate (all lanes)",
+                     "peak_source": peaks["source"],
+                     "algorithmic_bytes": "per query: its imported database + query + reply"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": top["achieved_qps"], "unit": "queries/s",
+                "h2d_bytes_per_step": top["h2d_bytes"] // top["queries"],
+                "d2h_bytes_per_step": top["d2h_bytes"] // top["queries"]},
+        "gpu_launches": sum(r["launches"] for r in results), "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    for d in imported.values():
+        d.free()
+    for c in ctxs:
+        c.close()
+    if mism:
+        log(f"{mism} served replies differ from the replies computed alone")
+        return 1
+    return 0
+
+
+def reference_serving_arm(args, w: dict, world: int, rank: int) -> int:
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    r = reference_mix(w, threads)
+    if "unavailable" in r:
+        print(json.dumps({"impl": "reference", "unavailable": r["unavailable"]}))
+        return 0
+    qps = r["qps"]
+    line = {"impl": "reference", "metric": METRIC, "value": round(qps, 4), "unit": "queries/s",
+            "n_gpus": args.gpus, "steps": 1, "warmup": 0, "ms_per_step": round(1e3 / qps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic: seeded uniform DB bytes; query from the reference's own PIRQueryGenerator",
+            "config": {"workload": w["desc"]},
+            "cpu_baseline": {"value": round(qps, 4), "unit": "queries/s", "cores": threads, "kind": "reference",
+                             "sample": f"one query per admitted shape on 1/{w['sample_div']} of its database, "
+                                       f"scaled, weighted as the arrivals; one query at a time",
+                             "per_shape": r["per_shape"]},
+            "e2e": {"value": round(qps, 4), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
 
 def main() -> int:
     ap = argparse.ArgumentParser()
@@ -529,6 +805,10 @@ def main() -> int:
     args = ap.parse_args()
     world, rank, local = dist_setup()
     w = dict(WORKLOADS[args.workload])
+    if args.workload == "serving":
+        if args.impl == "reference":
+            return reference_serving_arm(args, w, world, rank)
+        return serving_arm(args, w, world, rank, local)
     if args.workload == "batched":
         if args.impl == "reference":
             return reference_batched_arm(args, w, world, rank)

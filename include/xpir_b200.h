@@ -152,6 +152,34 @@ XPIR_B200_API int xpir_b200_reply_batch(xpir_b200_ctx *ctx, xpir_b200_request *r
 XPIR_B200_API int xpir_b200_autotune(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, const uint32_t *n,
                                      const void *query_dev, int *tile0);
 
+/* ---- serving loop ------------------------------------------------------------------ */
+/* A server over one or more contexts (one lane each: a worker thread and the context's
+ * stream, so lanes run concurrently on the GPU).  Queries wait in FIFO order per lane
+ * and are admitted while their device footprint (query, replies, recursion workspace)
+ * fits what is left of `device_budget_bytes`; each lane runs the admitted prefix (at
+ * most max_batch queries) as one xpir_b200_reply_batch, and queries that arrive
+ * meanwhile join the next batch.  No counterpart in the reference, whose server handles
+ * one query per session (apps/server/PIRSession.cpp:45-111, 467-565). */
+typedef struct xpir_b200_server xpir_b200_server;
+XPIR_B200_API int xpir_b200_server_create(xpir_b200_server **srv, xpir_b200_ctx *const *ctxs, uint32_t nctx,
+                                          uint64_t device_budget_bytes, uint32_t max_batch);
+/* Queues one query (host buffers; both must stay valid until xpir_b200_server_wait for
+ * the ticket returns).  XPIR_B200_ERR_NOMEM if its footprint exceeds the whole budget. */
+XPIR_B200_API int xpir_b200_server_submit(xpir_b200_server *srv, const xpir_b200_db *db, uint32_t d, const uint32_t *n,
+                                          const void *query, void *replies, uint64_t capacity_bytes, uint64_t *ticket);
+/* Waits for a query (timeout_ms < 0: no limit) and returns its status; latency is from
+ * submission to replies in host memory, queued_s from submission to admission.
+ * XPIR_B200_ERR_STATE if the ticket is unknown or not done within the timeout. */
+XPIR_B200_API int xpir_b200_server_wait(xpir_b200_server *srv, uint64_t ticket, int timeout_ms, uint64_t *nb_replies,
+                                        double *latency_s, double *queued_s);
+XPIR_B200_API int xpir_b200_server_stats(xpir_b200_server *srv, uint64_t *completed, uint64_t *batches,
+                                         uint64_t *max_batch, uint64_t *peak_device_bytes);
+/* Device bytes the server reserves while one query of this shape is admitted: its query
+ * and reply buffers and its share of the recursion workspace (for sizing budgets). */
+XPIR_B200_API int xpir_b200_server_footprint(const xpir_b200_db *db, uint32_t d, const uint32_t *n, uint64_t *bytes);
+/* Stops the lanes; call after every submitted query has been waited for. */
+XPIR_B200_API int xpir_b200_server_destroy(xpir_b200_server *srv);
+
 /* ---- reply without allocation ---------------------------------------------------- */
 /* Bytes of device scratch available to xpir_b200_reply_noalloc (64 MiB). */
 #define XPIR_B200_NOALLOC_SCRATCH_BYTES (64ull << 20)

@@ -1,0 +1,137 @@
+// Host-side check of the serving loop's admission and continuous batching
+// (xpir_b200/csrc/admission.h), compiled with g++ and driven by a fake executor:
+//   1. jobs run in FIFO order per lane and every job completes with the executor's status;
+//   2. the bytes admitted at once never exceed the budget;
+//   3. a job larger than the whole budget is refused at submission;
+//   4. jobs that arrive while a batch runs are admitted together in a later batch
+//      (continuous batching), never more than max_batch at a time;
+//   5. lanes run concurrently (two lanes' batches overlap in time);
+//   6. a head-of-line job that does not fit waits for memory rather than being skipped.
+#include <stdio.h>
+
+#include <atomic>
+#include <chrono>
+#include <thread>
+#include <vector>
+
+#include "../../xpir_b200/csrc/admission.h"
+
+#define CHECK(c)                                                \
+  do {                                                          \
+    if (!(c)) {                                                 \
+      printf("FAIL %s:%d: %s\n", __FILE__, __LINE__, #c);       \
+      return 1;                                                 \
+    }                                                           \
+  } while (0)
+
+namespace {
+
+struct Trace {
+  std::mutex mu;
+  std::vector<std::vector<uint64_t>> batches[2];  // tickets per batch, per lane
+  std::atomic<uint64_t> in_use{0}, peak{0};
+  std::atomic<int> active_lanes{0}, max_active_lanes{0};
+};
+
+}  // namespace
+
+int main() {
+  using xpir::Admission;
+  using xpir::Job;
+  Trace tr;
+  std::atomic<int> delay_ms{20};
+  const uint64_t budget = 1000;
+  Admission adm(2, budget, 4, [&](uint32_t lane, std::vector<Job *> &batch) {
+    uint64_t bytes = 0;
+    std::vector<uint64_t> ids;
+    for (Job *j : batch) {
+      bytes += j->footprint;
+      ids.push_back(j->ticket);
+    }
+    const uint64_t now = tr.in_use += bytes;
+    uint64_t pk = tr.peak.load();
+    while (now > pk && !tr.peak.compare_exchange_weak(pk, now)) {
+    }
+    const int a = ++tr.active_lanes;
+    int ma = tr.max_active_lanes.load();
+    while (a > ma && !tr.max_active_lanes.compare_exchange_weak(ma, a)) {
+    }
+    std::this_thread::sleep_for(std::chrono::milliseconds(delay_ms.load()));
+    --tr.active_lanes;
+    tr.in_use -= bytes;
+    {
+      std::lock_guard<std::mutex> lk(tr.mu);
+      tr.batches[lane].push_back(ids);
+    }
+    for (Job *j : batch) j->status = (int)(j->ticket % 7);  // executor-chosen status
+  });
+
+  // 3. Oversize refusal.
+  CHECK(adm.submit(0, budget + 1, nullptr) == 0);
+  CHECK(adm.submit(5, 1, nullptr) == 0);  // no such lane
+
+  // 1, 2, 4, 5. A burst on both lanes while the first batches run.
+  std::vector<uint64_t> tickets[2];
+  for (int i = 0; i < 40; i++)
+    for (uint32_t lane = 0; lane < 2; lane++) {
+      const uint64_t t = adm.submit(lane, 100 + 37 * (i % 5), nullptr);
+      CHECK(t != 0);
+      tickets[lane].push_back(t);
+    }
+  for (uint32_t lane = 0; lane < 2; lane++)
+    for (uint64_t t : tickets[lane]) {
+      Job *j = adm.wait(t, 20000);
+      CHECK(j != nullptr);
+      CHECK(j->done);
+      CHECK(j->status == (int)(t % 7));
+      CHECK(j->t_submit <= j->t_admit && j->t_admit <= j->t_done);
+      adm.release(t);
+    }
+  CHECK(adm.wait(tickets[0][0], 0) == nullptr);  // released: unknown now
+  const xpir::AdmissionStats st = adm.stats();
+  CHECK(st.completed == 80);
+  CHECK(st.refused == 2);
+  CHECK(st.peak_in_use <= budget);
+  CHECK(tr.peak.load() <= budget);
+  CHECK(st.max_batch_seen > 1 && st.max_batch_seen <= 4);  // batching happened, capped
+  CHECK(tr.max_active_lanes.load() == 2);                   // lanes overlapped
+  CHECK(adm.in_use() == 0);
+  {
+    std::lock_guard<std::mutex> lk(tr.mu);
+    for (int lane = 0; lane < 2; lane++) {
+      std::vector<uint64_t> order;
+      for (auto &b : tr.batches[lane]) order.insert(order.end(), b.begin(), b.end());
+      CHECK(order == tickets[lane]);  // FIFO per lane, each job exactly once
+    }
+  }
+
+  // 6. Head-of-line blocking by memory: a job needing the whole budget waits until the
+  // lane-1 jobs in flight release theirs, and the small job behind it (lane 0) is not
+  // admitted ahead of it.
+  delay_ms = 50;
+  const uint64_t a = adm.submit(1, 600, nullptr);
+  std::this_thread::sleep_for(std::chrono::milliseconds(10));
+  const uint64_t big = adm.submit(0, budget, nullptr);
+  const uint64_t small = adm.submit(0, 10, nullptr);
+  CHECK(a && big && small);
+  Job *ja = adm.wait(a, 20000);
+  Job *jb = adm.wait(big, 20000);
+  Job *js = adm.wait(small, 20000);
+  CHECK(ja && jb && js);
+  CHECK(jb->t_admit >= ja->t_done);  // waited for memory
+  CHECK(js->t_admit >= jb->t_admit);  // FIFO: not overtaken
+  adm.release(a);
+  adm.release(big);
+  adm.release(small);
+
+  // Timeout: a job that cannot finish within the wait's limit.
+  delay_ms = 300;
+  const uint64_t slow = adm.submit(0, 1, nullptr);
+  CHECK(adm.wait(slow, 10) == nullptr);
+  CHECK(adm.wait(slow, 20000) != nullptr);
+  adm.release(slow);
+  adm.stop();
+  CHECK(adm.submit(0, 1, nullptr) == 0);  // stopped: refused
+  printf("ok %llu batches\n", (unsigned long long)adm.stats().batches);
+  return 0;
+}

@@ -82,3 +82,15 @@ def test_shoup_factor_formula_host(tmp_path):
     out = subprocess.run([str(exe)], capture_output=True, text=True)
     assert out.returncode == 0, out.stdout + out.stderr
     assert out.stdout.startswith("ok")
+
+
+def test_admission_and_continuous_batching_host(tmp_path):
+    """The serving loop's queueing rules (xpir_b200/csrc/admission.h) under a fake executor:
+    FIFO per lane, budget never exceeded, oversize refused, batches formed from arrivals,
+    lanes concurrent, head-of-line job waits for memory."""
+    exe = tmp_path / "test_admission"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-pthread", "-o", str(exe),
+                    str(ROOT / "tests" / "cpp" / "test_admission.cpp")], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert out.stdout.startswith("ok")

@@ -1,0 +1,94 @@
+"""GPU tests of the serving loop (xpir_b200_server_*): queries from several clients on
+databases of two parameter sets, admitted by a device-memory budget and batched as they
+arrive.  Every served reply must be bit-identical to the single-query reply of the same
+query computed alone (integer work, no tolerance)."""
+from __future__ import annotations
+
+import threading
+
+import numpy as np
+import pytest
+
+from helpers import random_db, random_query
+
+pytestmark = pytest.mark.gpu
+
+
+def make_load(engine, ctxs):
+    """Databases on two parameter sets with d in {1, 2} and alpha in {1, 4}, and a list of
+    (db, n, host query, expected reply) of 4 queries per database."""
+    (ctx_a, (Na, ma)), (ctx_b, (Nb, mb)) = ctxs
+    specs = [(ctx_a, Na, ma, 900, 2000, [900], 1), (ctx_a, Na, ma, 900, 2000, [30, 30], 1),
+             (ctx_b, Nb, mb, 1200, 700, [300], 4), (ctx_b, Nb, mb, 1200, 700, [20, 15], 4)]
+    load, dbs = [], []
+    for k, (ctx, N, m, F, L, n, alpha) in enumerate(specs):
+        db = ctx.import_db(random_db(300 + k, F, L), F, L, alpha, engine.bits_per_coeff(N, m, n[0]))
+        dbs.append(db)
+        for j in range(4):
+            q = random_query(7000 + 10 * k + j, n, N, m, engine.moduli(m))
+            load.append((db, n, q, ctx.reply(db, n, q)))
+    return load, dbs
+
+
+def serve_all(engine, server, load, clients=4):
+    """Submits the load from `clients` threads at once; returns the replies by index."""
+    outs = [np.full(want.size, 0xDEAD, dtype=np.uint64) for (_, _, _, want) in load]
+    counts = [None] * len(load)
+    errors = []
+
+    def client(idx):
+        try:
+            tickets = [(i, server.submit(load[i][0], load[i][1], load[i][2], outs[i])) for i in idx]
+            for i, t in tickets:
+                counts[i] = server.wait(t, timeout_ms=60000)[0]
+        except Exception as e:  # reported below, in the test's thread
+            errors.append(e)
+
+    threads = [threading.Thread(target=client, args=(list(range(c, len(load), clients)),)) for c in range(clients)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    return outs, counts
+
+
+def test_served_replies_equal_replies_alone(engine):
+    with engine.Context(1024, 1) as ca, engine.Context(2048, 2) as cb:
+        load, _ = make_load(engine, [(ca, (1024, 1)), (cb, (2048, 2))])
+        with engine.Server([ca, cb], device_budget_bytes=1 << 30, max_batch=16) as srv:
+            outs, counts = serve_all(engine, srv, load)
+            st = srv.stats()
+        for (db, n, q, want), got, cnt in zip(load, outs, counts):
+            assert cnt * engine.ciphertext_bytes(db.ctx.N, db.ctx.m) == want.size * 8
+            assert np.array_equal(got, want)
+        assert st["completed"] == len(load)
+        assert st["max_batch"] >= 1
+
+
+def test_small_budget_queues_but_stays_exact(engine):
+    """A budget that admits about one query at a time: queries wait for memory, results
+    are unchanged, and the admitted bytes never exceed the budget."""
+    with engine.Context(1024, 1) as ca, engine.Context(2048, 2) as cb:
+        load, _ = make_load(engine, [(ca, (1024, 1)), (cb, (2048, 2))])
+        fp = [engine.Server.footprint(db, n) for (db, n, _, _) in load]
+        budget = max(fp) + min(fp) // 2  # the largest query fits, two large ones do not
+        with engine.Server([ca, cb], device_budget_bytes=budget, max_batch=8) as srv:
+            outs, _ = serve_all(engine, srv, load)
+            st = srv.stats()
+        for (_, _, _, want), got in zip(load, outs):
+            assert np.array_equal(got, want)
+        assert st["peak_device_bytes"] <= budget
+        assert st["completed"] == len(load)
+
+
+def test_oversize_query_refused(engine):
+    with engine.Context(1024, 1) as ca:
+        F, L = 500, 1000
+        db = ca.import_db(random_db(5, F, L), F, L, 1, engine.bits_per_coeff(1024, 1, F))
+        q = random_query(6, [F], 1024, 1, engine.moduli(1))
+        out = np.zeros(ca.reply(db, [F], q).size, dtype=np.uint64)
+        with engine.Server([ca], device_budget_bytes=4096) as srv:
+            with pytest.raises(engine.XpirError) as ei:
+                srv.submit(db, [F], q, out)
+            assert ei.value.status == engine.ERR_NOMEM

@@ -86,6 +86,15 @@ def _load():
                                       ctypes.c_int, ctypes.POINTER(c_u64)]
         L.xpir_b200_reply_batch.argtypes = [vp, ctypes.POINTER(Request), c_u32, ctypes.c_int]
         L.xpir_b200_autotune.argtypes = [vp, vp, c_u32, ctypes.POINTER(c_u32), vp, ctypes.POINTER(ctypes.c_int)]
+        L.xpir_b200_server_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), c_u32, c_u64, c_u32]
+        L.xpir_b200_server_submit.argtypes = [vp, vp, c_u32, ctypes.POINTER(c_u32), vp, vp, c_u64,
+                                              ctypes.POINTER(c_u64)]
+        L.xpir_b200_server_wait.argtypes = [vp, c_u64, ctypes.c_int, ctypes.POINTER(c_u64),
+                                            ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+        L.xpir_b200_server_stats.argtypes = [vp, ctypes.POINTER(c_u64), ctypes.POINTER(c_u64),
+                                             ctypes.POINTER(c_u64), ctypes.POINTER(c_u64)]
+        L.xpir_b200_server_destroy.argtypes = [vp]
+        L.xpir_b200_server_footprint.argtypes = [vp, c_u32, ctypes.POINTER(c_u32), ctypes.POINTER(c_u64)]
         _lib = L
     return _lib
 
@@ -276,3 +285,58 @@ class Context:
             self.close()
         except Exception:
             pass
+
+
+class Server:
+    """Serving loop over one or more contexts (xpir_b200_server_*): admission by a device
+    memory budget and continuous batching.  Query and reply buffers are host memory
+    (numpy arrays or pinned torch tensors) that must stay alive until wait() returns."""
+
+    def __init__(self, contexts: list[Context], device_budget_bytes: int, max_batch: int = 64):
+        arr = (ctypes.c_void_p * len(contexts))(*[c.handle.value for c in contexts])
+        h = ctypes.c_void_p()
+        _check(_load().xpir_b200_server_create(ctypes.byref(h), arr, len(contexts), device_budget_bytes, max_batch),
+               "server_create")
+        self.handle = h
+        self.contexts = contexts
+
+    def submit(self, db: Database, n: list[int], query, replies) -> int:
+        narr = (ctypes.c_uint32 * len(n))(*n)
+        cap = replies.nbytes if isinstance(replies, np.ndarray) else replies.numel() * replies.element_size()
+        t = ctypes.c_uint64()
+        _check(_load().xpir_b200_server_submit(self.handle, db.handle, len(n), narr, _ptr(query), _ptr(replies), cap,
+                                               ctypes.byref(t)), "server_submit")
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> tuple[int, float, float]:
+        """Returns (reply count, latency seconds, queued seconds)."""
+        cnt = ctypes.c_uint64()
+        lat = ctypes.c_double()
+        qd = ctypes.c_double()
+        _check(_load().xpir_b200_server_wait(self.handle, ticket, timeout_ms, ctypes.byref(cnt), ctypes.byref(lat),
+                                             ctypes.byref(qd)), "server_wait")
+        return cnt.value, lat.value, qd.value
+
+    @staticmethod
+    def footprint(db: Database, n: list[int]) -> int:
+        """Device bytes reserved while one query of this shape is admitted."""
+        narr = (ctypes.c_uint32 * len(n))(*n)
+        v = ctypes.c_uint64()
+        _check(_load().xpir_b200_server_footprint(db.handle, len(n), narr, ctypes.byref(v)), "server_footprint")
+        return v.value
+
+    def stats(self) -> dict:
+        v = [ctypes.c_uint64() for _ in range(4)]
+        _check(_load().xpir_b200_server_stats(self.handle, *[ctypes.byref(x) for x in v]), "server_stats")
+        return dict(zip(["completed", "batches", "max_batch", "peak_device_bytes"], [x.value for x in v]))
+
+    def close(self) -> None:
+        if self.handle:
+            _check(_load().xpir_b200_server_destroy(self.handle), "server_destroy")
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

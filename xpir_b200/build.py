@@ -17,7 +17,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libxpir_b200.so"
-SOURCES = ["params.cpp", "sm100_host.cu", "import.cu", "reply.cu", "capi.cu", "batch.cu", "noalloc.cu"]
+SOURCES = ["params.cpp", "sm100_host.cu", "import.cu", "reply.cu", "capi.cu", "batch.cu", "server.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -169,7 +169,8 @@ constexpr size_t kMaxPlans = 8;
 
 }  // namespace
 
-extern "C" int xpir_b200_reply_batch(xpir_b200_ctx *ctx, xpir_b200_request *reqs, uint32_t count, int use_graph) {
+int xpir::reply_batch_impl(xpir_b200_ctx *ctx, xpir_b200_request *reqs, uint32_t count, int use_graph,
+                           const WorkspaceFn *workspace) {
   if (!ctx || (!reqs && count)) return XPIR_B200_ERR_ARG;
   if (count == 0) return XPIR_B200_OK;
   std::lock_guard<std::mutex> lock(ctx->mu);
@@ -211,7 +212,8 @@ extern "C" int xpir_b200_reply_batch(xpir_b200_ctx *ctx, xpir_b200_request *reqs
   *ctx->status_host = 0;
 
   auto finish = [&](cudaError_t err) -> int {
-    if (err == cudaSuccess) err = cudaStreamSynchronize(ctx->stream);
+    const cudaError_t se = cudaStreamSynchronize(ctx->stream);  // also on error: nothing left in flight
+    if (err == cudaSuccess) err = se;
     int rc = status_of(err);
     if (rc == XPIR_B200_OK && *(volatile int *)ctx->status_host != 0) rc = XPIR_B200_ERR_TIMEOUT;
     for (const Group &g : groups)
@@ -223,34 +225,46 @@ extern "C" int xpir_b200_reply_batch(xpir_b200_ctx *ctx, xpir_b200_request *reqs
   };
 
   if (!use_graph) {
-    // Context workspaces, plus a task table sized for this submission.
-    void *dev_tasks = nullptr, *host_tasks = nullptr;
-    auto cleanup = [&]() {
-      cudaFree(dev_tasks);
-      if (host_tasks) cudaFreeHost(host_tasks);
-    };
-    if (z.ws_a > ctx->ws_a_bytes) {
-      cudaFree(ctx->ws_a);
-      ctx->ws_a = nullptr;
-      ctx->ws_a_bytes = 0;
-      if ((e = cudaMalloc(&ctx->ws_a, z.ws_a)) != cudaSuccess) return status_of(e);
-      ctx->ws_a_bytes = z.ws_a;
+    // Workspaces from the caller, or the context's own, grown on demand and kept; the
+    // task table likewise.  After the first calls an uncaptured batch allocates and frees
+    // nothing, so it never synchronises the device (other contexts' streams keep running).
+    void *wa = nullptr, *wb = nullptr;
+    if (workspace) {
+      if ((e = (*workspace)(z.ws_a, z.ws_b, &wa, &wb)) != cudaSuccess) return finish(e);
+    } else {
+      if (z.ws_a > ctx->ws_a_bytes) {
+        cudaFree(ctx->ws_a);
+        ctx->ws_a = nullptr;
+        ctx->ws_a_bytes = 0;
+        if ((e = cudaMalloc(&ctx->ws_a, z.ws_a)) != cudaSuccess) return finish(e);
+        ctx->ws_a_bytes = z.ws_a;
+      }
+      if (z.ws_b > ctx->ws_b_bytes) {
+        cudaFree(ctx->ws_b);
+        ctx->ws_b = nullptr;
+        ctx->ws_b_bytes = 0;
+        if ((e = cudaMalloc(&ctx->ws_b, z.ws_b)) != cudaSuccess) return finish(e);
+        ctx->ws_b_bytes = z.ws_b;
+      }
+      wa = ctx->ws_a;
+      wb = ctx->ws_b;
     }
-    if (z.ws_b > ctx->ws_b_bytes) {
-      cudaFree(ctx->ws_b);
-      ctx->ws_b = nullptr;
-      ctx->ws_b_bytes = 0;
-      if ((e = cudaMalloc(&ctx->ws_b, z.ws_b)) != cudaSuccess) return status_of(e);
-      ctx->ws_b_bytes = z.ws_b;
+    if (z.tasks > ctx->tasks_cap) {
+      cudaFree(ctx->tasks_dev);
+      if (ctx->tasks_host) cudaFreeHost(ctx->tasks_host);
+      ctx->tasks_dev = ctx->tasks_host = nullptr;
+      ctx->tasks_cap = 0;
+      const size_t cap = std::max<size_t>(z.tasks, 64);
+      e = cudaMalloc(&ctx->tasks_dev, cap * sizeof(ReplyTask));
+      if (e == cudaSuccess) e = cudaMallocHost(&ctx->tasks_host, cap * sizeof(ReplyTask));
+      if (e != cudaSuccess) return finish(e);
+      ctx->tasks_cap = cap;
     }
-    e = cudaMalloc(&dev_tasks, z.tasks * sizeof(ReplyTask));
-    if (e == cudaSuccess) e = cudaMallocHost(&host_tasks, z.tasks * sizeof(ReplyTask));
-    if (e == cudaSuccess)
-      e = enqueue(ctx, groups, reqs, (uint64_t *)ctx->ws_a, (uint64_t *)ctx->ws_b, (ReplyTask *)host_tasks,
-                  (ReplyTask *)dev_tasks);
-    const int rc = finish(e);
-    cleanup();
-    return rc;
+    // The pinned table may be rewritten here: the previous call on this context ended
+    // with a stream synchronisation, so its copy has completed.
+    e = enqueue(ctx, groups, reqs, (uint64_t *)wa, (uint64_t *)wb, (ReplyTask *)ctx->tasks_host,
+                (ReplyTask *)ctx->tasks_dev);
+    return finish(e);
   }
 
   // Graph path: replay a captured plan for the same request list, or capture one.
@@ -287,6 +301,10 @@ extern "C" int xpir_b200_reply_batch(xpir_b200_ctx *ctx, xpir_b200_request *reqs
   if (ctx->plans.size() >= kMaxPlans) ctx->plans.erase(ctx->plans.begin());
   ctx->plans.push_back(plan);
   return finish(cudaSuccess);
+}
+
+extern "C" int xpir_b200_reply_batch(xpir_b200_ctx *ctx, xpir_b200_request *reqs, uint32_t count, int use_graph) {
+  return reply_batch_impl(ctx, reqs, count, use_graph, nullptr);
 }
 
 extern "C" int xpir_b200_autotune(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, const uint32_t *n,

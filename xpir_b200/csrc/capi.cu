@@ -162,6 +162,8 @@ int xpir_b200_ctx_destroy(xpir_b200_ctx *ctx) {
   cudaFree(ctx->ws_query);
   cudaFree(ctx->ws_a);
   cudaFree(ctx->ws_b);
+  cudaFree(ctx->tasks_dev);
+  if (ctx->tasks_host) cudaFreeHost(ctx->tasks_host);
   ctx->plans.clear();
   if (ctx->status_host) cudaFreeHost(ctx->status_host);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);

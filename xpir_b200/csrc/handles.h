@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -33,6 +34,9 @@ struct xpir_b200_ctx {
   size_t ws_a_bytes = 0;
   void *ws_b = nullptr;  // re-imported level databases
   size_t ws_b_bytes = 0;
+  void *tasks_dev = nullptr;   // task table of uncaptured batches (device copy)
+  void *tasks_host = nullptr;  // and its pinned staging copy
+  size_t tasks_cap = 0;        // entries of both
   int *status_host = nullptr;  // kernel status word (mapped pinned memory)
   int *status_dev = nullptr;
   std::set<xpir_b200_db *> dbs;  // databases imported through this context
@@ -57,3 +61,18 @@ struct xpir_b200_db {
   uint64_t element_bytes = 0;
 };
 
+struct xpir_b200_request;
+
+namespace xpir {
+
+// Supplies the recursion workspace of an uncaptured batch: device buffers of at least
+// `a` bytes (level replies) and `b` bytes (re-imported level databases), valid in stream
+// order on the context's stream until the batch call returns.
+typedef std::function<cudaError_t(size_t a, size_t b, void **pa, void **pb)> WorkspaceFn;
+
+// xpir_b200_reply_batch with an optional workspace supplier (null: the context's own
+// cached workspaces).  Used by the serving loop to draw workspaces from its budgeted pool.
+int reply_batch_impl(xpir_b200_ctx *ctx, xpir_b200_request *reqs, uint32_t count, int use_graph,
+                     const WorkspaceFn *workspace);
+
+}  // namespace xpir
