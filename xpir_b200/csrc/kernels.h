@@ -71,12 +71,14 @@ struct alignas(128) ReplyTask {
 };
 
 // A compiled tile shape of the reply kernel: W coefficients per slice, C poly columns
-// per CTA, E slots per tile, NS pipeline stages, TB term buffers.
+// per CTA, E slots per tile, NS pipeline stages, TB term buffers, IPT slot pairs per
+// compute thread.
 struct TileShape {
-  int W, C, E, NS, TB;
+  int W, C, E, NS, TB, IPT;
 };
-// Index of the default shape for a level with P polys per element.
-int default_tile(uint64_t P);
+// Index of the default shape for a level with P polys per element, degree N, m moduli
+// and `ctas_per_slice` CTAs per (coefficient slice, modulus) (active groups x tasks).
+int default_tile(uint64_t P, uint32_t N, uint32_t m, uint64_t ctas_per_slice);
 // Shapes the autotuner may try for a level with P polys per element.
 std::vector<int> tile_candidates(uint64_t P);
 TileShape tile_shape(int tile);
@@ -91,7 +93,7 @@ cudaError_t launch_reply_tasks(const uint64_t *const *db, const uint64_t *const 
                                cudaStream_t stream, uint32_t *launches, int *status, int tile);
 
 // Whether the reply kernel supports this level shape (moduli with the fast Shoup-factor
-// path, degree a multiple of the slice width, 32-bit TMA coordinates).
+// path, degree a multiple of 16, 32-bit TMA coordinates).
 bool reply_level_supported(const ParamSet &ps, uint64_t n_real, uint64_t n_i, uint64_t groups);
 
 }  // namespace xpir

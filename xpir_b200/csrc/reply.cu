@@ -15,11 +15,12 @@
 //               (mbarrier expect-tx completion; slots past the real elements come back
 //               as zeros from the TMA out-of-bounds fill, which is exactly XPIR's
 //               zero-padding element).
-//   warps 1..8  compute: the query Shoup factors y' once per (slot, coefficient) from
-//               32-bit partial products (modarith.cuh), then the terms t for both
-//               ciphertext halves of all C columns into a double-buffered term tile.
-//   C warps     chains: one thread per (half, column, coefficient) consumes the term
-//               tiles strictly in slot order.
+//   compute     E*W/(2*IPT) threads, IPT slot pairs each: the query Shoup factors y'
+//               once per (slot, coefficient) from 32-bit partial products
+//               (modarith.cuh), then the terms t for both ciphertext halves of all C
+//               columns into a double-buffered term tile.
+//   chains      one thread per (half, column, coefficient) consumes the term tiles
+//               strictly in slot order.
 //
 // Every mbarrier wait is bounded; a wait that gives up sets the status word and the CTA
 // drains its in-flight copies and returns.
@@ -34,24 +35,15 @@
 #include "modarith.cuh"
 #include "sm100.cuh"
 
-// Single-column shape, chosen by a timing sweep on B200 over W in {8, 16, 32}, E in
-// {16..128}, NS in {2..8}, term buffers in {2, 4, 8} (the 100k x 4 KB workload).
-#ifndef XPIR_P1_W
-#define XPIR_P1_W 16
-#define XPIR_P1_E 64
-#define XPIR_P1_NS 3
-#define XPIR_P1_TB 2
-#endif
-
 namespace xpir {
 namespace {
 
 // Tile configuration: W coefficients per slice, C poly columns, E slots per tile, NS
-// pipeline stages.  One compute thread per slot pair of the tile; one chain thread per
-// (half, column, coefficient).
-template <int W, int C, int E, int NS, int TB = 2>
+// pipeline stages, TB term buffers, IPT slot pairs per compute thread and tile.  One
+// chain thread per (half, column, coefficient).
+template <int W, int C, int E, int NS, int TB = 2, int IPT = 1>
 struct Cfg {
-  static constexpr int kComputeWarps = E * W / 2 / 32;
+  static constexpr int kComputeWarps = E * W / 2 / 32 / IPT;
   static constexpr int kComputeThreads = 32 * kComputeWarps;
   static constexpr int kChainThreads = 2 * C * W;
   static constexpr int kChainWarps = (kChainThreads + 31) / 32;
@@ -61,7 +53,7 @@ struct Cfg {
   static constexpr int kT = 2 * C * E * W;  // terms     [half][C][E/2][W][2] per buffer
   static constexpr size_t kBytes = (size_t)(NS * (kX + kQ) + TB * kT) * 8 + (2 * NS + 2 * TB) * 8;
   static_assert((TB & (TB - 1)) == 0, "term buffers: a power of two");
-  static_assert(E % 2 == 0 && (E * W / 2) % 32 == 0, "slot pairs must fill whole warps");
+  static_assert(E % 2 == 0 && (E * W / 2) % (32 * IPT) == 0, "slot pairs must fill whole warps");
   static_assert((W * 8) % 16 == 0, "TMA rows must be multiples of 16 bytes");
 };
 
@@ -81,12 +73,14 @@ struct LevelShape {
 
 
 // The work of one CTA: group g, coefficient slice blockIdx.y, modulus / column block
-// blockIdx.z, with the DB and query tensor maps and the output of its task.
-template <int W, int C, int E, int NS, int TB>
+// blockIdx.z, with the DB and query tensor maps and the output of its task.  The last
+// slice may extend past N (W need not divide N): the TMA fills those coefficients with
+// zeros and their chains write nothing.
+template <int W, int C, int E, int NS, int TB, int IPT>
 __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUtensorMap *tm_q,
                                            uint64_t *__restrict__ out, const uint64_t g, const LevelShape &sh,
                                            const DevModuli &dm, int *status) {
-  using S = Cfg<W, C, E, NS, TB>;
+  using S = Cfg<W, C, E, NS, TB, IPT>;
   constexpr int kComputeWarps = S::kComputeWarps;
   constexpr int kComputeThreads = S::kComputeThreads;
   constexpr int kW = W;
@@ -154,10 +148,11 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
       const uint64_t *xst = xs + s * S::kX;
       const uint64_t *qst = qs + s * S::kQ;
       uint64_t *tb = terms + b * S::kT;
-      // Thread -> (coefficient k, slot pair e, e+1); the pair is stored as one 16-byte
-      // word so that a chain thread reads two consecutive slots with one load.
-      {
-        const int item = ct;
+      // Thread -> IPT items (coefficient k, slot pair e, e+1); the pair is stored as one
+      // 16-byte word so that a chain thread reads two consecutive slots with one load.
+#pragma unroll
+      for (int it = 0; it < IPT; it++) {
+        const int item = ct + it * kComputeThreads;
         const int k = item % kW, ep = item / kW, e = 2 * ep;
         const uint64_t ya0 = qst[(e * 2 + 0) * kW + k], yb0 = qst[(e * 2 + 1) * kW + k];
         const uint64_t ya1 = qst[(e * 2 + 2) * kW + k], yb1 = qst[(e * 2 + 3) * kW + k];
@@ -220,7 +215,7 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
       mbar_arrive(tempty + b);
     }
     const uint64_t cp = cp0 + col;
-    if (ok && cp < sh.P) {
+    if (ok && cp < sh.P && k0 + k < (int)sh.N) {
       const uint64_t mN = (uint64_t)sh.m * sh.N;
       out[((g * sh.P + cp) * 2 + h) * mN + (uint64_t)c * sh.N + k0 + k] = rop;
     }
@@ -231,24 +226,31 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
   }
 }
 
+// Two CTAs per SM for the narrow tiles (shared memory allows it), one for the wide ones.
+template <int W, int C, int E, int NS, int TB, int IPT>
+constexpr int min_blocks() {
+  return (C <= 2 && Cfg<W, C, E, NS, TB, IPT>::kThreads <= 640) ? 2 : 1;
+}
+
 // One query: tensor maps as grid constants.  Grid: x = group.
-template <int W, int C, int E, int NS, int TB>
-__global__ void __launch_bounds__(Cfg<W, C, E, NS, TB>::kThreads, C <= 2 ? 2 : 1)
+template <int W, int C, int E, int NS, int TB, int IPT>
+__global__ void __launch_bounds__(Cfg<W, C, E, NS, TB, IPT>::kThreads, min_blocks<W, C, E, NS, TB, IPT>())
     reply_tma_kernel(const __grid_constant__ CUtensorMap tm_db, const __grid_constant__ CUtensorMap tm_q,
                      uint64_t *__restrict__ out, const LevelShape sh, const DevModuli dm, int *status) {
-  reply_tile<W, C, E, NS, TB>(&tm_db, &tm_q, out, blockIdx.x, sh, dm, status);
+  reply_tile<W, C, E, NS, TB, IPT>(&tm_db, &tm_q, out, blockIdx.x, sh, dm, status);
 }
 
 // Several tasks of one level shape (a batch of queries): each task's tensor maps and
 // output come from a descriptor table in global memory.  Grid: x = group * tasks + task,
 // so the CTAs of all queries that read the same DB tile run side by side and share it
 // through L2.
-template <int W, int C, int E, int NS, int TB>
-__global__ void __launch_bounds__(Cfg<W, C, E, NS, TB>::kThreads, C <= 2 ? 2 : 1)
+template <int W, int C, int E, int NS, int TB, int IPT>
+__global__ void __launch_bounds__(Cfg<W, C, E, NS, TB, IPT>::kThreads, min_blocks<W, C, E, NS, TB, IPT>())
     reply_tma_tasks_kernel(const ReplyTask *__restrict__ tasks, const uint32_t ntasks, const LevelShape sh,
                            const DevModuli dm, int *status) {
   const uint32_t t = blockIdx.x % ntasks;
-  reply_tile<W, C, E, NS, TB>(&tasks[t].tm_db, &tasks[t].tm_q, tasks[t].out, blockIdx.x / ntasks, sh, dm, status);
+  reply_tile<W, C, E, NS, TB, IPT>(&tasks[t].tm_db, &tasks[t].tm_q, tasks[t].out, blockIdx.x / ntasks, sh, dm,
+                                   status);
 }
 
 // Tensor maps of one task for tile shape (W, C, E).
@@ -266,24 +268,24 @@ bool encode_task(const uint64_t *db, const uint64_t *query, uint64_t n_real, uin
          encode_tensor_map_u64_4d(tm_q, query, q_dims, q_strides, q_box);
 }
 
-template <int W, int C, int E, int NS, int TB>
+template <int W, int C, int E, int NS, int TB, int IPT>
 cudaError_t launch_c(const ReplyLevelArgs &a, const ParamSet &ps, const DevModuli &dm, uint64_t groups,
                      cudaStream_t stream, int *status) {
   CUtensorMap tm_db, tm_q;
   if (!encode_task<W, C, E>(a.db, a.query, a.n_real, a.P, a.n_i, ps, &tm_db, &tm_q)) return cudaErrorInvalidValue;
-  using S = Cfg<W, C, E, NS, TB>;
-  auto kern = reply_tma_kernel<W, C, E, NS, TB>;
+  using S = Cfg<W, C, E, NS, TB, IPT>;
+  auto kern = reply_tma_kernel<W, C, E, NS, TB, IPT>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kBytes);
   if (e != cudaSuccess) return e;
   const uint32_t col_blocks = (uint32_t)((a.P + C - 1) / C);
   LevelShape sh{a.n_real, a.P, a.n_i, ps.N, ps.m, col_blocks};
   if (groups > 0x7fffffffull || (uint64_t)ps.m * col_blocks > 65535) return cudaErrorInvalidValue;
-  dim3 grid((unsigned)groups, ps.N / W, (unsigned)(ps.m * col_blocks));
+  dim3 grid((unsigned)groups, (ps.N + W - 1) / W, (unsigned)(ps.m * col_blocks));
   kern<<<grid, S::kThreads, S::kBytes, stream>>>(tm_db, tm_q, a.out, sh, dm, status);
   return cudaGetLastError();
 }
 
-template <int W, int C, int E, int NS, int TB>
+template <int W, int C, int E, int NS, int TB, int IPT>
 cudaError_t launch_tasks_c(const uint64_t *const *db, const uint64_t *const *query, uint64_t *const *out,
                            uint32_t ntasks, uint64_t n_real, uint64_t P, uint64_t groups, uint64_t n_i,
                            const ParamSet &ps, const DevModuli &dm, ReplyTask *host_tasks, ReplyTask *dev_tasks,
@@ -295,14 +297,14 @@ cudaError_t launch_tasks_c(const uint64_t *const *db, const uint64_t *const *que
   }
   cudaError_t e = cudaMemcpyAsync(dev_tasks, host_tasks, ntasks * sizeof(ReplyTask), cudaMemcpyHostToDevice, stream);
   if (e != cudaSuccess) return e;
-  using S = Cfg<W, C, E, NS, TB>;
-  auto kern = reply_tma_tasks_kernel<W, C, E, NS, TB>;
+  using S = Cfg<W, C, E, NS, TB, IPT>;
+  auto kern = reply_tma_tasks_kernel<W, C, E, NS, TB, IPT>;
   e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kBytes);
   if (e != cudaSuccess) return e;
   const uint32_t col_blocks = (uint32_t)((P + C - 1) / C);
   LevelShape sh{n_real, P, n_i, ps.N, ps.m, col_blocks};
   if (groups * ntasks > 0x7fffffffull || (uint64_t)ps.m * col_blocks > 65535) return cudaErrorInvalidValue;
-  dim3 grid((unsigned)(groups * ntasks), ps.N / W, (unsigned)(ps.m * col_blocks));
+  dim3 grid((unsigned)(groups * ntasks), (ps.N + W - 1) / W, (unsigned)(ps.m * col_blocks));
   kern<<<grid, S::kThreads, S::kBytes, stream>>>(dev_tasks, ntasks, sh, dm, status);
   return cudaGetLastError();
 }
@@ -318,24 +320,46 @@ struct TileEntry {
   TasksFn tasks;
 };
 
-#define XPIR_TILE(W, C, E, NS, TB) \
-  { {W, C, E, NS, TB}, &launch_c<W, C, E, NS, TB>, &launch_tasks_c<W, C, E, NS, TB> }
+#define XPIR_TILE(W, C, E, NS, TB, IPT) \
+  { {W, C, E, NS, TB, IPT}, &launch_c<W, C, E, NS, TB, IPT>, &launch_tasks_c<W, C, E, NS, TB, IPT> }
 
-// Every compiled tile shape.  Entry 0..2: one poly column (the defaults and the
-// autotuner's alternatives for P = 1); then one entry per column count 2..8.
+// Every compiled tile shape.  Entries 0..2 are the one-column shapes for grids of at
+// most two CTAs per SM, picked by slice width (two slot pairs per compute thread);
+// entry 3 is the one-column shape for larger grids (one slot pair per thread: more
+// warps per SM); entries 4..5 are further one-column shapes for the autotuner; then one
+// entry per column count 2..8.  E, NS, TB come from timing sweeps on B200 over E in
+// {16..128}, NS in {2..8}, TB in {2, 4, 8}.
 const TileEntry kTiles[] = {
-    XPIR_TILE(XPIR_P1_W, 1, XPIR_P1_E, XPIR_P1_NS, XPIR_P1_TB),
-    XPIR_TILE(16, 1, 32, 4, 4),
-    XPIR_TILE(32, 1, 32, 3, 4),
-    XPIR_TILE(16, 2, 32, 3, 2),
-    XPIR_TILE(16, 3, 16, 4, 2),
-    XPIR_TILE(16, 4, 16, 3, 2),
-    XPIR_TILE(16, 5, 16, 3, 2),
-    XPIR_TILE(16, 6, 16, 3, 2),
-    XPIR_TILE(16, 7, 16, 3, 2),
-    XPIR_TILE(16, 8, 16, 3, 2),
+    XPIR_TILE(14, 1, 64, 3, 2, 2),
+    XPIR_TILE(16, 1, 64, 3, 2, 2),
+    XPIR_TILE(8, 1, 128, 3, 2, 2),
+    XPIR_TILE(16, 1, 64, 3, 2, 1),
+    XPIR_TILE(16, 1, 32, 4, 4, 1),
+    XPIR_TILE(32, 1, 32, 3, 4, 1),
+    XPIR_TILE(16, 2, 32, 3, 2, 1),
+    XPIR_TILE(16, 3, 16, 4, 2, 1),
+    XPIR_TILE(16, 4, 16, 3, 2, 1),
+    XPIR_TILE(16, 5, 16, 3, 2, 1),
+    XPIR_TILE(16, 6, 16, 3, 2, 1),
+    XPIR_TILE(16, 7, 16, 3, 2, 1),
+    XPIR_TILE(16, 8, 16, 3, 2, 1),
 };
 constexpr int kTileCount = sizeof(kTiles) / sizeof(kTiles[0]);
+constexpr int kFirstColumnTile = 6;  // entry of C = 2
+constexpr int kManyCtaTile = 3;      // one column, grids beyond two CTAs per SM
+
+// Streaming multiprocessors of the current device (cached per device).
+int sm_count() {
+  static int cache[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (cache[dev] == 0) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    cache[dev] = n;
+  }
+  return cache[dev];
+}
 
 }  // namespace
 
@@ -346,12 +370,35 @@ bool reply_level_supported(const ParamSet &ps, uint64_t n_real, uint64_t n_i, ui
   return ps.N % 16 == 0 && n_real < (1ull << 31) && groups * n_i + 256 < (1ull << 31);
 }
 
-int default_tile(uint64_t P) { return P <= 1 ? 0 : (int)(P >= 8 ? 9 : P + 1); }
+// One column per CTA: every CTA of a level does the same work (its slice width W times
+// the level's slots), and an SM's CTAs share its issue slots, so a grid of at most two
+// CTAs per SM takes about ceil(CTAs / SMs) * W.  The default takes the slice width that minimises this (the
+// widest on ties: longer TMA rows), e.g. W=14 for N=2048 and two moduli (294 CTAs on
+// 148 SMs against 256 for W=16, which leaves 40 SMs with half the work of the others).
+int default_tile(uint64_t P, uint32_t N, uint32_t m, uint64_t ctas_per_slice) {
+  if (P > 1) return kFirstColumnTile + (int)(P >= 8 ? 6 : P - 2);
+  const uint64_t sms = (uint64_t)sm_count();
+  int best = 1;
+  uint64_t best_cost = ~0ull, best_ctas = 0;
+  for (int t : {1, 0, 2}) {
+    const uint64_t W = (uint64_t)kTiles[t].shape.W;
+    const uint64_t ctas = ctas_per_slice * m * ((N + W - 1) / W);
+    const uint64_t cost = (ctas + sms - 1) / sms * W;
+    if (cost < best_cost) {
+      best = t;
+      best_cost = cost;
+      best_ctas = ctas;
+    }
+  }
+  // Several waves of CTAs: the SMs stay evenly loaded anyway, and more warps per CTA
+  // hide more latency (measured on the recursive and batched workloads).
+  return best_ctas > 2 * sms ? kManyCtaTile : best;
+}
 
 std::vector<int> tile_candidates(uint64_t P) {
-  if (P <= 1) return {0, 1, 2};
+  if (P <= 1) return {0, 1, 2, 3, 4, 5};
   // several columns per CTA (query factors shared) or one column per CTA
-  return {default_tile(P), 0};
+  return {default_tile(P, 0, 0, 0), kManyCtaTile};
 }
 
 TileShape tile_shape(int tile) { return kTiles[tile].shape; }
@@ -374,7 +421,8 @@ cudaError_t launch_reply_tasks(const uint64_t *const *db, const uint64_t *const 
   }
   if (active == 0) return cudaSuccess;
   if (!reply_level_supported(ps, n_real, n_i, active * ntasks)) return cudaErrorNotSupported;
-  if (tile < 0 || tile >= kTileCount || kTiles[tile].shape.C > (int)(P > 8 ? 8 : P)) tile = default_tile(P);
+  if (tile < 0 || tile >= kTileCount || kTiles[tile].shape.C > (int)(P > 8 ? 8 : P))
+    tile = default_tile(P, ps.N, ps.m, active * ntasks);
   if (launches) (*launches)++;
   return kTiles[tile].tasks(db, query, out, ntasks, n_real, P, active, n_i, ps, dm, host_tasks, dev_tasks, stream,
                             status);
@@ -395,7 +443,8 @@ cudaError_t launch_reply_level(const ReplyLevelArgs &a, const ParamSet &ps, cons
   if (active == 0) return cudaSuccess;
   if (!reply_level_supported(ps, a.n_real, a.n_i, active)) return cudaErrorNotSupported;
   if (launches) (*launches)++;
-  if (tile < 0 || tile >= kTileCount || kTiles[tile].shape.C > (int)(a.P > 8 ? 8 : a.P)) tile = default_tile(a.P);
+  if (tile < 0 || tile >= kTileCount || kTiles[tile].shape.C > (int)(a.P > 8 ? 8 : a.P))
+    tile = default_tile(a.P, ps.N, ps.m, active);
   return kTiles[tile].single(a, ps, dm, active, stream, status);
 }
 
