@@ -1,6 +1,7 @@
 // Host-side check of the engine's modular arithmetic (xpir_b200/csrc/modarith.cuh),
 // compiled with g++: the division-free Shoup factor must equal floor(y*2^64/p) mod 2^64
-// (the reference's u128 division, PIRReplyGeneratorNFL_internal.cpp:764) for every y.
+// (the reference's u128 division, PIRReplyGeneratorNFL_internal.cpp:764) for every y, and
+// the accumulate forms (given 2^64 - p) must equal the plain ones.
 #include <stdio.h>
 #include <stdlib.h>
 
@@ -29,8 +30,13 @@ int main() {
       const uint64_t want = (uint64_t)(((unsigned __int128)y << 64) / p);
       const uint64_t got = xpir::shoup_factor(y, p, s.k, s.delta);
       const uint64_t got8 = xpir::shoup_factor8(y, p, (uint32_t)s.delta);
+      const uint64_t got8n = xpir::shoup_factor8_np(y, p, 0 - p, (uint32_t)s.delta);
+      // The accumulate form of the lazy product equals the subtract form for any x.
+      const uint64_t x = rng();
+      const uint64_t lazy = xpir::shoup_lazy(x, y, want, p);
+      const uint64_t lazy_np = xpir::shoup_lazy_np(x, y, want, 0 - p);
       checked++;
-      if (want != got || want != got8) {
+      if (want != got || want != got8 || want != got8n || lazy != lazy_np) {
         printf("mismatch p=%llu y=%llu want=%llu got=%llu\n", (unsigned long long)p, (unsigned long long)y,
                (unsigned long long)want, (unsigned long long)got);
         exit(1);

@@ -36,6 +36,22 @@ XPIR_HD uint64_t shoup_lazy(uint64_t x, uint64_t y, uint64_t ys, uint64_t p) {
   return x * y - mulhi(x, ys) * p;
 }
 
+// The same product given np = 2^64 - p: x*y + q*np (mod 2^64), so that the second
+// product accumulates onto the first in multiply-add instructions.  Device code passes
+// np through opaque() so that the compiler keeps this form instead of rewriting it back
+// into a product and a subtraction.
+XPIR_HD uint64_t shoup_lazy_np(uint64_t x, uint64_t y, uint64_t ys, uint64_t np) {
+  return x * y + mulhi(x, ys) * np;
+}
+
+// A value the compiler cannot see through (a register move on the device).
+XPIR_HD uint64_t opaque(uint64_t v) {
+#if defined(__CUDA_ARCH__)
+  asm volatile("mov.b64 %0, %0;" : "+l"(v));
+#endif
+  return v;
+}
+
 // mulmodShoup (crypto/NFLlib.hpp:282-289): the lazy product with one conditional
 // subtraction.
 XPIR_HD uint64_t shoup_mul(uint64_t x, uint64_t y, uint64_t ys, uint64_t p) {
@@ -112,6 +128,16 @@ XPIR_HD uint64_t shoup_factor8(uint64_t y, uint64_t p, uint32_t delta) {
   const uint32_t q0 = (uint32_t)((B + (A >> 32)) >> 29);
   const uint64_t zlo = A + (B << 32);
   const uint64_t rem = zlo - (uint64_t)q0 * p;
+  return (y << 3) + q0 + (rem >= p ? 1u : 0u);
+}
+
+// shoup_factor8 with np = 2^64 - p supplied (see shoup_lazy_np): the remainder
+// z - q0*p is formed as z + q0*np.
+XPIR_HD uint64_t shoup_factor8_np(uint64_t y, uint64_t p, uint64_t np, uint32_t delta) {
+  const uint64_t A = (uint64_t)(uint32_t)y * delta;
+  const uint64_t B = (uint64_t)(uint32_t)(y >> 32) * delta;
+  const uint32_t q0 = (uint32_t)((B + (A >> 32)) >> 29);
+  const uint64_t rem = A + (B << 32) + (uint64_t)q0 * np;
   return (y << 3) + q0 + (rem >= p ? 1u : 0u);
 }
 

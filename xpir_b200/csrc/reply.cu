@@ -65,6 +65,11 @@ __device__ __forceinline__ void lds_v2(const uint64_t *p, uint64_t &a, uint64_t 
 __device__ __forceinline__ void sts_v2(uint64_t *p, uint64_t a, uint64_t b) {
   asm volatile("st.shared.v2.u64 [%0], {%1, %2};\n" ::"r"(smem_addr(p)), "l"(a), "l"(b) : "memory");
 }
+// The same store as plain C++, which the compiler may schedule freely (the mbarrier
+// arrive that publishes the tile orders it).
+__device__ __forceinline__ void st_v2(uint64_t *p, uint64_t a, uint64_t b) {
+  *reinterpret_cast<ulonglong2 *>(p) = make_ulonglong2(a, b);
+}
 
 struct LevelShape {
   uint64_t n_real, P, n_i;
@@ -97,6 +102,7 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
   const uint32_t cp0 = (blockIdx.z - c * sh.col_blocks) * C;
   const uint64_t p = dm.p[c];
   const uint32_t delta = (uint32_t)dm.shoup_delta[c];
+  const uint64_t np = opaque(0 - p);
   const uint32_t tiles = (uint32_t)((sh.n_i + E - 1) / E);
 
   if (threadIdx.x == 0) {
@@ -150,21 +156,45 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
       uint64_t *tb = terms + b * S::kT;
       // Thread -> IPT items (coefficient k, slot pair e, e+1); the pair is stored as one
       // 16-byte word so that a chain thread reads two consecutive slots with one load.
+      // Several columns: all inputs are loaded before the arithmetic, so the loads of
+      // later columns overlap the products of earlier ones (faster for C > 1 on B200;
+      // for one column the interleaved form below is slightly faster).
+      if constexpr (C > 1) {
 #pragma unroll
-      for (int it = 0; it < IPT; it++) {
-        const int item = ct + it * kComputeThreads;
-        const int k = item % kW, ep = item / kW, e = 2 * ep;
-        const uint64_t ya0 = qst[(e * 2 + 0) * kW + k], yb0 = qst[(e * 2 + 1) * kW + k];
-        const uint64_t ya1 = qst[(e * 2 + 2) * kW + k], yb1 = qst[(e * 2 + 3) * kW + k];
-        const uint64_t ysa0 = shoup_factor8(ya0, p, delta), ysb0 = shoup_factor8(yb0, p, delta);
-        const uint64_t ysa1 = shoup_factor8(ya1, p, delta), ysb1 = shoup_factor8(yb1, p, delta);
+        for (int it = 0; it < IPT; it++) {
+          const int item = ct + it * kComputeThreads;
+          const int k = item % kW, ep = item / kW, e = 2 * ep;
+          uint64_t x[C][2];
+          const uint64_t ya0 = qst[(e * 2 + 0) * kW + k], yb0 = qst[(e * 2 + 1) * kW + k];
+          const uint64_t ya1 = qst[(e * 2 + 2) * kW + k], yb1 = qst[(e * 2 + 3) * kW + k];
 #pragma unroll
-        for (int col = 0; col < C; col++) {
-          const uint64_t x0 = xst[(e * C + col) * kW + k], x1 = xst[((e + 1) * C + col) * kW + k];
-          sts_v2(tb + (((0 * C + col) * (E / 2) + ep) * kW + k) * 2, shoup_lazy(x0, ya0, ysa0, p),
-                 shoup_lazy(x1, ya1, ysa1, p));
-          sts_v2(tb + (((1 * C + col) * (E / 2) + ep) * kW + k) * 2, shoup_lazy(x0, yb0, ysb0, p),
-                 shoup_lazy(x1, yb1, ysb1, p));
+          for (int col = 0; col < C; col++) {
+            x[col][0] = xst[(e * C + col) * kW + k];
+            x[col][1] = xst[((e + 1) * C + col) * kW + k];
+          }
+          const uint64_t ysa0 = shoup_factor8_np(ya0, p, np, delta), ysb0 = shoup_factor8_np(yb0, p, np, delta);
+          const uint64_t ysa1 = shoup_factor8_np(ya1, p, np, delta), ysb1 = shoup_factor8_np(yb1, p, np, delta);
+#pragma unroll
+          for (int col = 0; col < C; col++) {
+            const uint64_t x0 = x[col][0], x1 = x[col][1];
+            st_v2(tb + (((0 * C + col) * (E / 2) + ep) * kW + k) * 2, shoup_lazy_np(x0, ya0, ysa0, np),
+                  shoup_lazy_np(x1, ya1, ysa1, np));
+            st_v2(tb + (((1 * C + col) * (E / 2) + ep) * kW + k) * 2, shoup_lazy_np(x0, yb0, ysb0, np),
+                  shoup_lazy_np(x1, yb1, ysb1, np));
+          }
+        }
+      } else {
+#pragma unroll
+        for (int it = 0; it < IPT; it++) {
+          const int item = ct + it * kComputeThreads;
+          const int k = item % kW, ep = item / kW, e = 2 * ep;
+          const uint64_t ya0 = qst[(e * 2 + 0) * kW + k], yb0 = qst[(e * 2 + 1) * kW + k];
+          const uint64_t ya1 = qst[(e * 2 + 2) * kW + k], yb1 = qst[(e * 2 + 3) * kW + k];
+          const uint64_t ysa0 = shoup_factor8_np(ya0, p, np, delta), ysb0 = shoup_factor8_np(yb0, p, np, delta);
+          const uint64_t ysa1 = shoup_factor8_np(ya1, p, np, delta), ysb1 = shoup_factor8_np(yb1, p, np, delta);
+          const uint64_t x0 = xst[e * kW + k], x1 = xst[(e + 1) * kW + k];
+          sts_v2(tb + (ep * kW + k) * 2, shoup_lazy_np(x0, ya0, ysa0, np), shoup_lazy_np(x1, ya1, ysa1, np));
+          sts_v2(tb + (((E / 2) + ep) * kW + k) * 2, shoup_lazy_np(x0, yb0, ysb0, np), shoup_lazy_np(x1, yb1, ysb1, np));
         }
       }
       mbar_arrive(empty + s);
