@@ -357,8 +357,9 @@ struct TileEntry {
 // most two CTAs per SM, picked by slice width (two slot pairs per compute thread);
 // entry 3 is the one-column shape for larger grids (one slot pair per thread: more
 // warps per SM); entries 4..5 are further one-column shapes for the autotuner; then one
-// entry per column count 2..8.  E, NS, TB come from timing sweeps on B200 over E in
-// {16..128}, NS in {2..8}, TB in {2, 4, 8}.
+// entry per column count 2..8 with 16-coefficient slices, and the same with 8 (twice
+// the CTAs, for levels whose grid would not fill the GPU).  E, NS, TB come from timing
+// sweeps on B200 over E in {16..128}, NS in {2..8}, TB in {2, 4, 8}.
 const TileEntry kTiles[] = {
     XPIR_TILE(14, 1, 64, 3, 2, 2),
     XPIR_TILE(16, 1, 64, 3, 2, 2),
@@ -373,9 +374,17 @@ const TileEntry kTiles[] = {
     XPIR_TILE(16, 6, 16, 3, 2, 1),
     XPIR_TILE(16, 7, 16, 3, 2, 1),
     XPIR_TILE(16, 8, 16, 3, 2, 1),
+    XPIR_TILE(8, 2, 32, 3, 2, 1),
+    XPIR_TILE(8, 3, 32, 3, 2, 1),
+    XPIR_TILE(8, 4, 32, 3, 2, 1),
+    XPIR_TILE(8, 5, 32, 3, 2, 1),
+    XPIR_TILE(8, 6, 32, 3, 2, 1),
+    XPIR_TILE(8, 7, 32, 3, 2, 1),
+    XPIR_TILE(8, 8, 32, 3, 2, 1),
 };
 constexpr int kTileCount = sizeof(kTiles) / sizeof(kTiles[0]);
-constexpr int kFirstColumnTile = 6;  // entry of C = 2
+constexpr int kFirstColumnTile = 6;        // entry of C = 2, W = 16
+constexpr int kFirstNarrowColumnTile = 13;  // entry of C = 2, W = 8
 constexpr int kManyCtaTile = 3;      // one column, grids beyond two CTAs per SM
 
 // Streaming multiprocessors of the current device (cached per device).
@@ -406,8 +415,19 @@ bool reply_level_supported(const ParamSet &ps, uint64_t n_real, uint64_t n_i, ui
 // widest on ties: longer TMA rows), e.g. W=14 for N=2048 and two moduli (294 CTAs on
 // 148 SMs against 256 for W=16, which leaves 40 SMs with half the work of the others).
 int default_tile(uint64_t P, uint32_t N, uint32_t m, uint64_t ctas_per_slice) {
-  if (P > 1) return kFirstColumnTile + (int)(P >= 8 ? 6 : P - 2);
   const uint64_t sms = (uint64_t)sm_count();
+  if (P > 1) {
+    // C columns per CTA; 16- or 8-coefficient slices by the same cost (the 1,000 x 12 KB
+    // level at N=1024: 64 CTAs of W=16 against 128 of W=8, which run 1.7x faster).
+    const int C = (int)(P >= 8 ? 8 : P);
+    const int wide = kFirstColumnTile + C - 2, narrow = kFirstNarrowColumnTile + C - 2;
+    if (N == 0) return wide;
+    const uint64_t col_blocks = (P + C - 1) / C;
+    const uint64_t ctas16 = ctas_per_slice * m * ((N + 15) / 16) * col_blocks;
+    const uint64_t ctas8 = ctas_per_slice * m * ((N + 7) / 8) * col_blocks;
+    const uint64_t cost16 = (ctas16 + sms - 1) / sms * 16, cost8 = (ctas8 + sms - 1) / sms * 8;
+    return cost8 < cost16 ? narrow : wide;
+  }
   int best = 1;
   uint64_t best_cost = ~0ull, best_ctas = 0;
   for (int t : {1, 0, 2}) {
@@ -427,8 +447,10 @@ int default_tile(uint64_t P, uint32_t N, uint32_t m, uint64_t ctas_per_slice) {
 
 std::vector<int> tile_candidates(uint64_t P) {
   if (P <= 1) return {0, 1, 2, 3, 4, 5};
-  // several columns per CTA (query factors shared) or one column per CTA
-  return {default_tile(P, 0, 0, 0), kManyCtaTile};
+  // several columns per CTA (query factors shared), 16- or 8-coefficient slices, or
+  // one column per CTA
+  const int C = (int)(P >= 8 ? 8 : P);
+  return {kFirstColumnTile + C - 2, kFirstNarrowColumnTile + C - 2, kManyCtaTile};
 }
 
 TileShape tile_shape(int tile) { return kTiles[tile].shape; }
