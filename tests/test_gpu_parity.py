@@ -153,7 +153,9 @@ def test_launch_count_and_reuse(engine, oracle):
             q = random_query(100 + s, n, N, m, oracle.moduli(m))
             rep = ctx.reply(d, n, q)
             assert np.array_equal(rep, oracle.reply(imp, F, P, n, q, b, N, m))
-        assert ctx.launch_count - before == 3 * 3  # per reply: 2 level kernels + 1 re-import
+        # per reply: the level-0 query factors (4 groups share each slot), 2 level kernels
+        # and 1 re-import
+        assert ctx.launch_count - before == 3 * 4
 
 
 def test_context_close_releases_databases(engine, oracle):

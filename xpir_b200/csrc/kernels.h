@@ -54,6 +54,9 @@ struct ReplyLevelArgs {
   uint64_t n_i;
   const uint64_t *query;  // [n_i][2][m][N]
   uint64_t *out;
+  // The query's Shoup factors (same layout), from launch_query_factors, or null to derive
+  // them in the kernel.  Used by one-poly levels (P = 1).
+  const uint64_t *query_factors = nullptr;
 };
 // `status` is a device-visible int that a kernel sets to a nonzero KernelStatus when one
 // of its bounded waits gives up (sm100.cuh); the caller clears and reads it.
@@ -67,14 +70,16 @@ cudaError_t launch_reply_level(const ReplyLevelArgs &a, const ParamSet &ps, cons
 struct alignas(128) ReplyTask {
   CUtensorMap tm_db;
   CUtensorMap tm_q;
+  CUtensorMap tm_qf;  // query factors (tiles that read them)
   uint64_t *out;
 };
 
 // A compiled tile shape of the reply kernel: W coefficients per slice, C poly columns
 // per CTA, E slots per tile, NS pipeline stages, TB term buffers, IPT slot pairs per
-// compute thread.
+// compute thread, pre: reads precomputed query factors.
 struct TileShape {
   int W, C, E, NS, TB, IPT;
+  bool pre;
 };
 // Index of the default shape for a level with P polys per element, degree N, m moduli
 // and `ctas_per_slice` CTAs per (coefficient slice, modulus) (active groups x tasks).
@@ -87,10 +92,26 @@ int tile_count();
 // `ntasks` reply levels of the same shape (n_real, P, n_groups, n_i), one per query,
 // in one launch.  `host_tasks` (pinned, ntasks entries) is filled here and copied to
 // `dev_tasks` on `stream` before the launch.  tile < 0 picks the default shape.
-cudaError_t launch_reply_tasks(const uint64_t *const *db, const uint64_t *const *query, uint64_t *const *out,
-                               uint32_t ntasks, uint64_t n_real, uint64_t P, uint64_t n_groups, uint64_t n_i,
-                               const ParamSet &ps, const DevModuli &dm, ReplyTask *host_tasks, ReplyTask *dev_tasks,
-                               cudaStream_t stream, uint32_t *launches, int *status, int tile);
+cudaError_t launch_reply_tasks(const uint64_t *const *db, const uint64_t *const *query,
+                               const uint64_t *const *factors, uint64_t *const *out, uint32_t ntasks, uint64_t n_real,
+                               uint64_t P, uint64_t n_groups, uint64_t n_i, const ParamSet &ps, const DevModuli &dm,
+                               ReplyTask *host_tasks, ReplyTask *dev_tasks, cudaStream_t stream, uint32_t *launches,
+                               int *status, int tile);
+
+// Groups of a level that hold at least one real element (the others reply exactly zero).
+inline uint64_t active_groups(uint64_t n_real, uint64_t n_i, uint64_t n_groups) {
+  const uint64_t a = n_i == 0 ? 0 : (n_real + n_i - 1) / n_i;
+  return a < n_groups ? a : n_groups;
+}
+
+// Whether a level should read precomputed query factors: one poly per element and at
+// least four groups sharing each query slot, so that deriving every factor once (one
+// memory-bound pass) replaces deriving it once per group inside the reply kernel.
+inline bool level_uses_factors(uint64_t P, uint64_t active) { return P == 1 && active >= 4; }
+
+// The Shoup factors of n_ct query ciphertexts into `factors` (same layout and size).
+cudaError_t launch_query_factors(const uint64_t *query, uint64_t *factors, uint64_t n_ct, const ParamSet &ps,
+                                 const DevModuli &dm, cudaStream_t stream, uint32_t *launches);
 
 // Whether the reply kernel supports this level shape (moduli with the fast Shoup-factor
 // path, degree a multiple of 16, 32-bit TMA coordinates).
