@@ -335,7 +335,7 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
                         traffic = int(line.split("=")[1])
             roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                         "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
-                        "kernel": "reply_level_kernel", "peak_source": peaks["source"],
+                        "kernel": "reply_tma_kernel", "peak_source": peaks["source"],
                         "algorithmic_bytes_per_launch": algo_bytes, "kernel_ms": round(kern_ms, 4)}
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
