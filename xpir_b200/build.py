@@ -17,6 +17,8 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libxpir_b200.so"
+PIR_LIB = PKG / "libxpir_b200_pir.so"  # the libpir-shaped C++ API (host code over the C ABI)
+PIR_SOURCES = ["host/pir_reply_generator.cpp"]
 SOURCES = ["params.cpp", "sm100_host.cu", "import.cu", "reply.cu", "capi.cu", "batch.cu", "server.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -50,7 +52,23 @@ def build(force: bool = False, extra: list[str] | None = None, verbose: bool = F
     return LIB
 
 
+def build_pir(force: bool = False) -> Path:
+    """The C++ API of include/xpir_b200_pir.hpp: host code only, linked against the engine
+    library next to it (rpath $ORIGIN)."""
+    srcs = [PKG / s for s in PIR_SOURCES]
+    headers = [ROOT / "include" / "xpir_b200_pir.hpp", ROOT / "include" / "xpir_b200.h"]
+    if not force and PIR_LIB.exists() and PIR_LIB.stat().st_mtime >= max(p.stat().st_mtime for p in srcs + headers):
+        return PIR_LIB
+    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-Wall", "-I", str(ROOT / "include"), "-o", str(PIR_LIB),
+           *map(str, srcs), "-L", str(PKG), "-l:libxpir_b200.so", "-Wl,-rpath,$ORIGIN"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"g++ failed:\n{res.stdout}\n{res.stderr}")
+    return PIR_LIB
+
+
 if __name__ == "__main__":
     verbose = "-v" in sys.argv
     extra = ["-Xptxas", "-v"] if "--ptxas" in sys.argv else None
     print(build(force=True, extra=extra, verbose=verbose or bool(extra)))
+    print(build_pir(force=True))
