@@ -131,14 +131,17 @@ XPIR_HD uint64_t shoup_factor8(uint64_t y, uint64_t p, uint32_t delta) {
   return (y << 3) + q0 + (rem >= p ? 1u : 0u);
 }
 
-// shoup_factor8 with np = 2^64 - p supplied (see shoup_lazy_np): the remainder
-// z - q0*p is formed as z + q0*np.
+// shoup_factor8 with np = 2^64 - p supplied (see shoup_lazy_np).  The correction
+// [z - q0*p >= p] is read from the sign of r = z - (q0+1)*p = z + (q0+1)*np: since
+// z - q0*p lies in [0, 2p) and 2p < 2^63, r is negative (top bit set) exactly when no
+// correction is due.  Three instructions fewer than the compare on B200.
 XPIR_HD uint64_t shoup_factor8_np(uint64_t y, uint64_t p, uint64_t np, uint32_t delta) {
+  (void)p;
   const uint64_t A = (uint64_t)(uint32_t)y * delta;
   const uint64_t B = (uint64_t)(uint32_t)(y >> 32) * delta;
-  const uint32_t q0 = (uint32_t)((B + (A >> 32)) >> 29);
-  const uint64_t rem = A + (B << 32) + (uint64_t)q0 * np;
-  return (y << 3) + q0 + (rem >= p ? 1u : 0u);
+  const uint32_t q1 = (uint32_t)((B + (A >> 32)) >> 29) + 1;
+  const uint64_t r = A + (B << 32) + (uint64_t)q1 * np;
+  return (y << 3) + (q1 - (uint32_t)(r >> 63));
 }
 
 }  // namespace xpir
