@@ -69,6 +69,12 @@ def lib():
         L.xo_reply.argtypes = [_u64p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32,
                                ctypes.POINTER(ctypes.c_uint32), _u64p, ctypes.c_uint32, ctypes.c_uint32,
                                ctypes.c_uint32, _u64p]
+        L.xo_decrypt.argtypes = [_u64p, _u64p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _u8p]
+        L.xo_extract_count.restype = ctypes.c_uint64
+        L.xo_extract_count.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                       ctypes.c_uint32]
+        L.xo_extract.argtypes = [_u64p, ctypes.c_uint64, _u64p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                 ctypes.c_uint32, ctypes.c_uint64, _u8p]
         L.xo_reply_count.restype = ctypes.c_uint64
         L.xo_reply_count.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                      ctypes.c_uint32, ctypes.c_uint32]
@@ -189,6 +195,28 @@ def reply(db: np.ndarray, n_real: int, P: int, n: list[int], query: np.ndarray, 
     return out
 
 
+def decrypt(ct: np.ndarray, sk: np.ndarray, b: int, N: int, m: int) -> np.ndarray:
+    """b*N/8 plaintext bytes of one ciphertext (NFLLWE::dec + decrypt)."""
+    out = np.zeros(b * N // 8, dtype=np.uint8)
+    c = np.ascontiguousarray(ct, dtype=np.uint64)
+    k = np.ascontiguousarray(sk, dtype=np.uint64)
+    assert lib().xo_decrypt(_p64(c), _p64(k), b, N, m, _p8(out)) == 0
+    return out
+
+
+def extract_count(agg_bytes: int, lvl: int, b: int, N: int, m: int) -> int:
+    return int(lib().xo_extract_count(agg_bytes, lvl, b, N, m))
+
+
+def extract(replies: np.ndarray, sk: np.ndarray, d: int, b: int, N: int, m: int, agg_bytes: int) -> np.ndarray:
+    """The aggregated element (agg_bytes) recovered from d-level replies."""
+    out = np.zeros(agg_bytes, dtype=np.uint8)
+    r = np.ascontiguousarray(replies, dtype=np.uint64)
+    k = np.ascontiguousarray(sk, dtype=np.uint64)
+    assert lib().xo_extract(_p64(r), r.size // (2 * m * N), _p64(k), d, b, N, m, agg_bytes, _p8(out)) == 0
+    return out
+
+
 def reply_count(L: int, alpha: int, d: int, b: int, N: int, m: int) -> int:
     return int(lib().xo_reply_count(L, alpha, d, b, N, m))
 
@@ -263,6 +291,14 @@ def ref_extract(N: int, m: int, n: list[int], alpha: int, L: int, keyseed: int, 
         _ref("extract", {"params": params_str(N, m), "alpha": alpha, "d": len(n), "n": ",".join(map(str, n)),
                          "eltbytes": L, "keyseed": keyseed, "reply-in": t / "r.bin", "plain-out": t / "p.bin"})
         return np.fromfile(t / "p.bin", dtype=np.uint8)
+
+
+def ref_key(N: int, m: int, keyseed: int) -> np.ndarray:
+    """The reference's seeded secret key, [m][N] in the NTT domain."""
+    with tempfile.TemporaryDirectory() as td:
+        t = Path(td)
+        _ref("key", {"params": params_str(N, m), "keyseed": keyseed, "key-out": t / "k.bin"})
+        return np.fromfile(t / "k.bin", dtype=np.uint64)
 
 
 def ref_info(N: int, m: int, n0: int) -> dict:

@@ -10,6 +10,7 @@
 // Commands (all binary files are raw little-endian):
 //   run      full PIR round trip; dumps query, imported DB, replies, recovered element
 //   extract  decrypt a given reply (e.g. one produced on the GPU) with the seeded key
+//   key      write the seeded secret key (NTT domain) for the oracle's and GPU's decryption
 //   tables   dump the NTT tables built by NFLlib::configureNTT (crypto/NFLlib.cpp:44-194)
 //   bitsplit NFLlib::bitsplitter (+CRT) output, before the NTT (crypto/NFLlib.cpp:846-876)
 //   deser    NFLlib::deserializeDataNFL output (bitsplit + CRT + nttAndPowPhi)
@@ -303,6 +304,18 @@ int cmd_extract(const Args &a) {
   return 0;
 }
 
+// The seeded secret key (NFLLWE::secretKey, crypto/NFLLWE.cpp:98-120): m*N words, NTT
+// domain, written to --key-out.
+int cmd_key(const Args &a) {
+  PIRParameters params = pir_params(a);
+  HomomorphicCrypto *crypto = make_crypto(a, params);
+  NFLLWE *lwe = dynamic_cast<NFLLWE *>(crypto);
+  const uint64_t words = (uint64_t)lwe->getnbModuli() * lwe->getpolyDegree();
+  write_file(a.str("key-out"), lwe->getsecretKey()[0], words * 8);
+  delete crypto;
+  return 0;
+}
+
 int cmd_info(const Args &a) {
   PIRParameters params = pir_params(a);
   HomomorphicCrypto *crypto = make_crypto(a, params);
@@ -405,7 +418,7 @@ int cmd_ntt(const Args &a) {
 
 int main(int argc, char **argv) {
   if (argc < 2) {
-    fprintf(stderr, "usage: xpir_ref run|extract|tables|bitsplit|deser|ntt|info [--key value ...]\n");
+    fprintf(stderr, "usage: xpir_ref run|extract|key|tables|bitsplit|deser|ntt|info [--key value ...]\n");
     return 2;
   }
   std::string cmd = argv[1];
@@ -424,6 +437,7 @@ int main(int argc, char **argv) {
   if (cmd == "deser") return cmd_bitsplit(a, true);
   if (cmd == "ntt") return cmd_ntt(a);
   if (cmd == "info") return cmd_info(a);
+  if (cmd == "key") return cmd_key(a);
   fprintf(stderr, "xpir_ref: unknown command %s\n", cmd.c_str());
   return 2;
 }

@@ -493,3 +493,158 @@ uint64_t xo_reply_count(uint64_t element_bytes, uint32_t alpha, uint32_t d, uint
   for (uint32_t i = 1; i < d; i++) out = (unsigned int)ceil(out * (double)ct_bytes / (double)abs_bytes);
   return out;
 }
+
+/* ---- client-side decryption and extraction ---------------------------------------- */
+
+static uint64_t powmod(uint64_t a, uint64_t e, uint64_t p) {
+  uint64_t r = 1;
+  a %= p;
+  while (e) {
+    if (e & 1) r = mulmod(r, a, p);
+    a = mulmod(a, a, p);
+    e >>= 1;
+  }
+  return r;
+}
+
+/* Multi-word helpers (little-endian 64-bit limbs, XO_LIMBS of them). */
+#define XO_LIMBS 6
+static uint64_t limbs_mod(const uint64_t *x, uint64_t p) {
+  u128 r = 0;
+  for (int i = XO_LIMBS - 1; i >= 0; i--) r = ((r << 64) | x[i]) % p;
+  return (uint64_t)r;
+}
+static void limbs_muladd(uint64_t *x, const uint64_t *M, uint64_t v) { /* x += M*v */
+  u128 carry = 0;
+  for (int i = 0; i < XO_LIMBS; i++) {
+    u128 t = (u128)M[i] * v + x[i] + carry;
+    x[i] = (uint64_t)t;
+    carry = t >> 64;
+  }
+}
+static void limbs_mul_small(uint64_t *M, uint64_t v) { /* M *= v */
+  u128 carry = 0;
+  for (int i = 0; i < XO_LIMBS; i++) {
+    u128 t = (u128)M[i] * v + carry;
+    M[i] = (uint64_t)t;
+    carry = t >> 64;
+  }
+}
+static int limbs_cmp(const uint64_t *a, const uint64_t *b) {
+  for (int i = XO_LIMBS - 1; i >= 0; i--)
+    if (a[i] != b[i]) return a[i] > b[i] ? 1 : -1;
+  return 0;
+}
+
+/* NFLLWE::dec + NFLLWE::decrypt for one ciphertext (crypto/NFLLWE.cpp:375-475, 515-551):
+ * per modulus m_c = submod(b_c, mulandaddShoup(0, a_c, s_c), p_c) (NFLlib.hpp:255-267,
+ * 303-321), inverse NTT and N^-1 phi^-i (NFLlib.hpp:613-626), then per coefficient the CRT
+ * lift x in [0, P) (NFLlib.cpp:504-532; computed here by mixed radix, which gives the same
+ * unique x), centred: x - P when 2x > P, and its low b bits, serialised LSB-first
+ * (NFLlib.cpp:412-495).  out receives b*N/8 bytes. */
+int xo_decrypt(const uint64_t *ct, const uint64_t *sk, uint32_t b, uint32_t N, uint32_t m, uint8_t *out) {
+  if (!valid_shape(N, m) || b == 0 || b >= 128 || (uint64_t)b >= 61ull * m) return -1;
+  uint64_t *tab = (uint64_t *)malloc(xo_tables_words(N, m) * 8);
+  uint64_t *mm = (uint64_t *)malloc((size_t)m * N * 8);
+  if (!tab || !mm) {
+    free(tab);
+    free(mm);
+    return -2;
+  }
+  xo_tables(N, m, tab);
+  for (uint32_t c = 0; c < m; c++) {
+    const uint64_t p = tab[(uint64_t)c * (1 + 8 * (uint64_t)N)];
+    const uint64_t *a = ct + (uint64_t)c * N, *bb = ct + ((uint64_t)m + c) * N, *s = sk + (uint64_t)c * N;
+    for (uint32_t i = 0; i < N; i++) {
+      const uint64_t temp = mac_shoup(0, a[i], s[i], shoup(s[i], p), p);
+      const uint64_t y = (temp < p) ? p - temp : p - temp % p;
+      uint64_t z = bb[i] + y;
+      z -= (z >= p) ? p : 0;
+      mm[(uint64_t)c * N + i] = z;
+    }
+  }
+  xo_intt_phi(mm, 1, N, m);
+  /* CRT constants: P, and for mixed radix the prefix products and their inverses. */
+  uint64_t P[XO_LIMBS] = {1}, Mi[XO_MAX_MODULI][XO_LIMBS], inv[XO_MAX_MODULI];
+  for (uint32_t c = 0; c < m; c++) {
+    const uint64_t p = xo_modulus(c);
+    memcpy(Mi[c], P, sizeof(P));
+    inv[c] = c ? powmod(limbs_mod(P, p), p - 2, p) : 1;
+    limbs_mul_small(P, p);
+  }
+  memset(out, 0, (size_t)b * N / 8);
+  for (uint32_t i = 0; i < N; i++) {
+    uint64_t x[XO_LIMBS] = {0};
+    for (uint32_t c = 0; c < m; c++) {
+      const uint64_t p = xo_modulus(c);
+      const uint64_t r = mm[(uint64_t)c * N + i] % p;
+      const uint64_t have = limbs_mod(x, p);
+      const uint64_t v = mulmod((r + p - have) % p, inv[c], p);
+      limbs_muladd(x, Mi[c], v);
+    }
+    uint64_t x2[XO_LIMBS];
+    uint64_t carry = 0;
+    for (int k = 0; k < XO_LIMBS; k++) {
+      x2[k] = (x[k] << 1) | carry;
+      carry = x[k] >> 63;
+    }
+    uint64_t lo = x[0], hi = x[1];
+    if (limbs_cmp(x2, P) > 0) { /* x - P mod 2^128 */
+      const u128 d = (((u128)x[1] << 64) | x[0]) - (((u128)P[1] << 64) | P[0]);
+      lo = (uint64_t)d;
+      hi = (uint64_t)(d >> 64);
+    }
+    /* low b bits at bit offset i*b */
+    const uint64_t pos = (uint64_t)i * b;
+    for (uint32_t k = 0; k < b; k++) {
+      const uint64_t bit = k < 64 ? (lo >> k) & 1 : (hi >> (k - 64)) & 1;
+      if (bit) out[(pos + k) >> 3] |= (uint8_t)(1u << ((pos + k) & 7));
+    }
+  }
+  free(tab);
+  free(mm);
+  return 0;
+}
+
+/* Ciphertexts decrypted at recursion level lvl (1 = the innermost) for an aggregated
+ * element of agg_bytes: PIRReplyExtraction_internal::extractReply's float arithmetic
+ * (pir/replyExtraction/PIRReplyExtraction_internal.cpp:50-58). */
+uint64_t xo_extract_count(uint64_t agg_bytes, uint32_t lvl, uint32_t b, uint32_t N, uint32_t m) {
+  const float abs_bytes = (float)((uint64_t)b * N / 8), ct_bytes = (float)(16ull * m * N);
+  uint64_t nbr = (uint64_t)ceilf((float)agg_bytes / abs_bytes);
+  for (uint32_t i = 1; i < lvl; i++) nbr = (uint64_t)ceilf((float)nbr * ct_bytes / abs_bytes);
+  return nbr;
+}
+
+/* PIRReplyExtraction_internal::extractReply (…_internal.cpp:41-106): from level d down
+ * to 1, decrypt that level's ciphertexts (the replies at d; below, the previous level's
+ * plaintext bytes read as ciphertexts); the level-1 plaintexts concatenated give the
+ * aggregated element, of which agg_bytes are written to out. */
+int xo_extract(const uint64_t *replies, uint64_t nb_replies, const uint64_t *sk, uint32_t d, uint32_t b, uint32_t N,
+               uint32_t m, uint64_t agg_bytes, uint8_t *out) {
+  const uint64_t abs_bytes = (uint64_t)b * N / 8, ct_words = 2ull * m * N;
+  if (d == 0 || abs_bytes == 0) return -1;
+  if (nb_replies < xo_extract_count(agg_bytes, d, b, N, m)) return -1;
+  uint8_t *in = NULL; /* plaintext of the level above, read as ciphertexts */
+  for (uint32_t lvl = d; lvl >= 1; lvl--) {
+    const uint64_t nbr = xo_extract_count(agg_bytes, lvl, b, N, m);
+    uint8_t *plain = (uint8_t *)calloc(nbr * abs_bytes + 8, 1);
+    if (!plain) {
+      free(in);
+      return -2;
+    }
+    for (uint64_t j = 0; j < nbr; j++) {
+      const uint64_t *c = lvl == d ? replies + j * ct_words : (const uint64_t *)(in + j * ct_words * 8);
+      if (xo_decrypt(c, sk, b, N, m, plain + j * abs_bytes) != 0) {
+        free(plain);
+        free(in);
+        return -1;
+      }
+    }
+    free(in);
+    in = plain;
+  }
+  memcpy(out, in, agg_bytes);
+  free(in);
+  return 0;
+}

@@ -101,6 +101,20 @@ uint64_t xo_reply(const uint64_t *db, uint64_t n_real, uint64_t P, uint32_t d, c
  * pir/replyGenerator/PIRReplyGeneratorNFL_internal.cpp:667-679). */
 uint64_t xo_reply_count(uint64_t element_bytes, uint32_t alpha, uint32_t d, uint32_t b, uint32_t N, uint32_t m);
 
+/* Client-side decryption of one ciphertext with the secret key sk ([m][N], NTT domain,
+ * as NFLLWE::secretKey holds it): b*N/8 plaintext bytes (crypto/NFLLWE.cpp:375-475,
+ * 515-551). */
+int xo_decrypt(const uint64_t *ct, const uint64_t *sk, uint32_t b, uint32_t N, uint32_t m, uint8_t *out);
+
+/* Ciphertexts decrypted at recursion level lvl for agg_bytes of aggregated element
+ * (PIRReplyExtraction_internal.cpp:50-58). */
+uint64_t xo_extract_count(uint64_t agg_bytes, uint32_t lvl, uint32_t b, uint32_t N, uint32_t m);
+
+/* Reply extraction for d levels (PIRReplyExtraction_internal.cpp:41-106): agg_bytes of
+ * the aggregated element into out.  0 on success. */
+int xo_extract(const uint64_t *replies, uint64_t nb_replies, const uint64_t *sk, uint32_t d, uint32_t b, uint32_t N,
+               uint32_t m, uint64_t agg_bytes, uint8_t *out);
+
 #ifdef __cplusplus
 }
 #endif

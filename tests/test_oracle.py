@@ -123,3 +123,35 @@ def test_reference_extraction_recovers_element(ref):
     r = ref.ref_run(1024, 1, [12], 1, db, 12, 2000, keyseed=9, chosen=7)
     assert r["extract_ok"] == 1
     assert np.array_equal(r["plain"], db[7 * 2000:8 * 2000])
+
+
+@pytest.mark.parametrize("N,m,n,alpha,L,reduced", [
+    (1024, 1, [20], 1, 900, True), (2048, 3, [8], 2, 700, True), (1024, 2, [6, 5], 1, 400, True),
+    (512, 1, [4, 4, 3], 1, 300, True), (1024, 2, [12], 1, 600, False)])
+def test_extraction_matches_reference(ref, N, m, n, alpha, L, reduced):
+    """Decryption and multi-level extraction of arbitrary ciphertexts (words below 2p as
+    replies have them, or any 64-bit words) equal the reference's PIRReplyExtraction with
+    the same seeded key, byte for byte."""
+    rng = np.random.default_rng(N + m + L)
+    d, b = len(n), ref.bits_per_coeff(N, m, n[0])
+    key = ref.ref_key(N, m, 9)
+    nct = ref.extract_count(L * alpha, d, b, N, m)
+    ct = rng.integers(0, 2**64, size=(nct, 2, m, N), dtype=np.uint64)
+    if reduced:
+        for c, p in enumerate(ref.moduli(m)):
+            ct[:, :, c, :] %= np.uint64(2 * p)
+    ct = ct.reshape(-1)
+    assert np.array_equal(ref.extract(ct, key, d, b, N, m, L * alpha), ref.ref_extract(N, m, n, alpha, L, 9, ct))
+
+
+def test_extraction_round_trip_with_reference_key(ref):
+    """The reference answers its own query; the restatement, given the reference's secret
+    key, recovers the chosen aggregated element from that reply."""
+    N, m, n, alpha, F, L, chosen = 1024, 2, [5, 4], 2, 37, 600, 13
+    db = np.random.default_rng(12).integers(0, 256, size=F * L, dtype=np.uint8)
+    r = ref.ref_run(N, m, n, alpha, db, F, L, keyseed=21, chosen=chosen)
+    key = ref.ref_key(N, m, 21)
+    b = ref.bits_per_coeff(N, m, n[0])
+    got = ref.extract(r["reply"], key, len(n), b, N, m, L * alpha)
+    assert np.array_equal(got, db[chosen * alpha * L:(chosen + 1) * alpha * L])
+    assert np.array_equal(got, r["plain"])
