@@ -152,6 +152,26 @@ XPIR_B200_API int xpir_b200_reply_batch(xpir_b200_ctx *ctx, xpir_b200_request *r
 XPIR_B200_API int xpir_b200_autotune(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, const uint32_t *n,
                                      const void *query_dev, int *tile0);
 
+/* ---- reply extraction (client side) ------------------------------------------------ */
+/* Ciphertexts decrypted at recursion level `level` (1 = innermost) for an aggregated
+ * element of aggregated_bytes (alpha * element bytes): the float arithmetic of
+ * PIRReplyExtraction_internal::extractReply (pir/replyExtraction/PIRReplyExtraction_internal.cpp:50-58).
+ * At level d this is the number of replies to pass to xpir_b200_extract. */
+XPIR_B200_API uint64_t xpir_b200_extract_count(uint64_t aggregated_bytes, uint32_t level, uint32_t bits_per_coeff,
+                                               uint32_t poly_degree, uint32_t nb_moduli);
+/* Decrypts d-level replies with the client's secret key and recovers the aggregated
+ * element: PIRReplyExtraction::extractReply + popPlaintextResult (pir/libpir.cpp:171-201,
+ * PIRReplyExtraction_internal.cpp:41-106) with NFLLWE::decrypt (crypto/NFLLWE.cpp:375-475,
+ * 515-551), on the GPU.  secret_key: host memory, [nb_moduli][poly_degree] u64 words in the
+ * NTT domain, as NFLLWE keeps its secretKey.  replies: xpir_b200_extract_count(..., d, ...)
+ * ciphertexts (host memory unless replies_on_device).  The first aggregated_bytes bytes
+ * of the element are written to plaintext (host memory unless out_on_device).  Supports
+ * up to 4 moduli (fewer than 128 bits per coefficient). */
+XPIR_B200_API int xpir_b200_extract(xpir_b200_ctx *ctx, const uint64_t *secret_key, uint32_t d, uint32_t bits_per_coeff,
+                                    uint64_t aggregated_bytes, const void *replies, uint64_t nb_replies,
+                                    int replies_on_device, void *plaintext, uint64_t capacity_bytes,
+                                    int out_on_device);
+
 /* ---- serving loop ------------------------------------------------------------------ */
 /* A server over one or more contexts (one lane each: a worker thread and the context's
  * stream, so lanes run concurrently on the GPU).  Queries wait in FIFO order per lane

@@ -86,6 +86,10 @@ def _load():
                                       ctypes.c_int, ctypes.POINTER(c_u64)]
         L.xpir_b200_reply_batch.argtypes = [vp, ctypes.POINTER(Request), c_u32, ctypes.c_int]
         L.xpir_b200_autotune.argtypes = [vp, vp, c_u32, ctypes.POINTER(c_u32), vp, ctypes.POINTER(ctypes.c_int)]
+        L.xpir_b200_extract_count.restype = c_u64
+        L.xpir_b200_extract_count.argtypes = [c_u64, c_u32, c_u32, c_u32, c_u32]
+        L.xpir_b200_extract.argtypes = [vp, vp, c_u32, c_u32, c_u64, vp, c_u64, ctypes.c_int, vp, c_u64,
+                                        ctypes.c_int]
         L.xpir_b200_server_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), c_u32, c_u64, c_u32]
         L.xpir_b200_server_submit.argtypes = [vp, vp, c_u32, ctypes.POINTER(c_u32), vp, vp, c_u64,
                                               ctypes.POINTER(c_u64)]
@@ -132,6 +136,11 @@ def reply_count(element_bytes: int, alpha: int, d: int, b: int, N: int, m: int) 
 
 def ciphertext_bytes(N: int, m: int) -> int:
     return int(_load().xpir_b200_ciphertext_bytes(N, m))
+
+
+def extract_count(aggregated_bytes: int, level: int, b: int, N: int, m: int) -> int:
+    """Ciphertexts decrypted at recursion level `level` (the reply count at level d)."""
+    return int(_load().xpir_b200_extract_count(aggregated_bytes, level, b, N, m))
 
 
 def modulus(i: int) -> int:
@@ -258,6 +267,20 @@ class Context:
         status = _load().xpir_b200_reply_batch(self.handle, reqs, len(items), int(use_graph))
         _check(status, "reply_batch")
         return [r.nb_replies for r in reqs]
+
+    def extract(self, secret_key: np.ndarray, d: int, b: int, aggregated_bytes: int, replies, out=None):
+        """Client-side extraction on the GPU: the aggregated element (aggregated_bytes) from
+        d-level replies, with the secret key ([m][N] u64, NTT domain).  `replies` and `out`
+        may be numpy (host) or torch CUDA tensors; returns `out` (a new uint8 array if None)."""
+        sk = np.ascontiguousarray(secret_key, dtype=np.uint64)
+        if out is None:
+            out = np.zeros(aggregated_bytes, dtype=np.uint8)
+        cap = out.nbytes if isinstance(out, np.ndarray) else out.numel() * out.element_size()
+        nrep = (replies.nbytes if isinstance(replies, np.ndarray) else replies.numel() * replies.element_size())
+        nrep //= 16 * self.m * self.N
+        _check(_load().xpir_b200_extract(self.handle, sk.ctypes.data, d, b, aggregated_bytes, _ptr(replies), nrep,
+                                         _on_device(replies), _ptr(out), cap, _on_device(out)), "extract")
+        return out
 
     def autotune(self, db: Database, n: list[int], query) -> int:
         """Times the compiled tile shapes on this query's shape and keeps the fastest."""
