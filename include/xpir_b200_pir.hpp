@@ -1,6 +1,7 @@
-// xpir_b200_pir.hpp -- C++ server-side API of the B200 reply engine, shaped like XPIR's
-// libpir (libpir.hpp:101-169, pir/libpir.cpp:77-163) so that a server written against
-// libpir's PIRReplyGenerator moves over by changing its includes and namespace.
+// xpir_b200_pir.hpp -- C++ API of the B200 reply engine, shaped like XPIR's libpir
+// (libpir.hpp:101-210, pir/libpir.cpp:77-201) so that a server written against libpir's
+// PIRReplyGenerator (or a client using its PIRReplyExtraction) moves over by changing its
+// includes and namespace.
 //
 // The classes sit on the C ABI of include/xpir_b200.h.  Semantics kept from libpir:
 //   * pushQuery takes ownership of a malloc'd query ciphertext (freed by freeQueries);
@@ -150,8 +151,7 @@ class PIRReplyGenerator {
   bool popReply(char **reply);
   uint64_t getnbRepliesGenerated() const { return nb_replies_; }
   uint64_t getReplyElementBytesize() const { return crypto_.getCiphertextBytesize(); }
-  // Device bytes generateReplyGeneric may give one chunk's imported polys (default:
-  // a quarter of the device memory free when the generator was created).
+  // Device bytes generateReplyGeneric may give one chunk's imported polys (default 16 GiB).
   void setDeviceMemoryBudget(uint64_t bytes) { budget_ = bytes; }
 
  private:
@@ -165,6 +165,35 @@ class PIRReplyGenerator {
   std::vector<char *> queries_;
   std::vector<uint64_t> replies_;  // nb_replies_ ciphertexts, contiguous
   uint64_t nb_replies_ = 0, next_reply_ = 0, budget_ = 0;
+};
+
+// libpir's PIRReplyExtraction (libpir.hpp:176-210, pir/libpir.cpp:165-201), client side,
+// decrypting on the GPU with the client's secret key ([nb_moduli][poly_degree] words in
+// the NTT domain, as XPIR's NFLLWE holds it).
+class PIRReplyExtraction {
+ public:
+  PIRReplyExtraction(PIRParameters &param, HomomorphicCrypto &cryptoMethod, std::vector<uint64_t> secret_key,
+                     int device = 0);
+  ~PIRReplyExtraction();
+  // One reply ciphertext (malloc'd; the extractor owns it).
+  void pushEncryptedReply(char *rawBytes);
+  // Decrypts the pushed replies down to the element of maxFileBytesize bytes (times alpha).
+  void extractReply(uint64_t maxFileBytesize);
+  // The next plaintext chunk of getPlaintextReplyBytesize() bytes (malloc'd; the caller
+  // frees it); false after getnbPlaintextReplies chunks.  The bytes past the aggregated
+  // element in the last chunk read as zeros.
+  bool popPlaintextResult(char **result);
+  uint64_t getPlaintextReplyBytesize() const;
+  uint64_t getnbPlaintextReplies(uint64_t maxFileBytesize) const;
+
+ private:
+  PIRParameters param_;
+  HomomorphicCrypto &crypto_;
+  std::vector<uint64_t> key_;
+  std::shared_ptr<xpir_b200_ctx> ctx_;
+  std::vector<char *> replies_;
+  std::vector<char> plain_;
+  uint64_t chunks_ = 0, next_ = 0;
 };
 
 }  // namespace xpir_b200

@@ -9,7 +9,9 @@
 //       reads <dir>/params.txt ("crypto alpha d n0 .. n{d-1} budget"), <dir>/sizes.bin
 //       (u64 per element: its byte length), <dir>/db.bin (the elements back to back) and
 //       <dir>/query.bin; writes <dir>/reply.bin (generateReply) and
-//       <dir>/reply_generic.bin (generateReplyGeneric under the given device budget).
+//       <dir>/reply_generic.bin (generateReplyGeneric under the given device budget);
+//       with <dir>/key.bin present, PIRReplyExtraction decrypts the reply with that key
+//       into <dir>/plain.bin (popPlaintextResult chunks, concatenated).
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -153,6 +155,28 @@ int run_mode(const std::string &dir) {
   std::vector<char> generic = pop_all(gen2);
   CHECK(generic.size() == gen2.getnbRepliesGenerated() * ct);
   CHECK(spill(dir + "/reply_generic.bin", generic));
+  const std::vector<char> keybytes = slurp(dir + "/key.bin");
+  if (!keybytes.empty()) {
+    std::vector<uint64_t> key(keybytes.size() / 8);
+    memcpy(key.data(), keybytes.data(), key.size() * 8);
+    PIRReplyExtraction ex(params, *crypto, key);
+    for (uint64_t i = 0; i * ct < reply.size(); i++) {
+      char *r = (char *)malloc(ct);  // ownership passes to the extractor
+      memcpy(r, reply.data() + i * ct, ct);
+      ex.pushEncryptedReply(r);
+    }
+    ex.extractReply(db.getmaxFileBytesize());
+    std::vector<char> plain;
+    char *chunk;
+    uint64_t chunks = 0;
+    while (ex.popPlaintextResult(&chunk)) {
+      plain.insert(plain.end(), chunk, chunk + ex.getPlaintextReplyBytesize());
+      free(chunk);
+      chunks++;
+    }
+    CHECK(chunks == ex.getnbPlaintextReplies(db.getmaxFileBytesize()));
+    CHECK(spill(dir + "/plain.bin", plain));
+  }
   printf("ok run replies=%llu generic=%llu kept=%d\n", (unsigned long long)count,
          (unsigned long long)gen2.getnbRepliesGenerated(), kept ? 1 : 0);
   return 0;

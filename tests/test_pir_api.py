@@ -85,3 +85,23 @@ def test_pir_api_recursive_aggregated_equals_oracle(pir_exe, oracle, engine, tmp
     assert np.array_equal(rep, want)
     assert np.array_equal(gen, want)
     assert "kept=1" in line
+
+
+@pytest.mark.gpu
+def test_pir_api_server_and_client_round_trip(pir_exe, ref, engine, tmp_path):
+    """The reference's client builds the query (seeded key); the C++ API answers it
+    (PIRReplyGenerator) and decrypts the answer with the same key (PIRReplyExtraction):
+    the chosen element comes back, and the reply equals the reference's own."""
+    N, m, n, alpha, F, L, chosen = 1024, 2, [7, 6], 2, 80, 900, 23
+    db = np.random.default_rng(51).integers(0, 256, size=F * L, dtype=np.uint8)
+    r = ref.ref_run(N, m, n, alpha, db, F, L, keyseed=77, chosen=chosen, extract=False)
+    (tmp_path / "params.txt").write_text(f"LWE:80:{N}:{60 * m} {alpha} {len(n)} {' '.join(map(str, n))} {1 << 30}\n")
+    (tmp_path / "sizes.bin").write_bytes(np.full(F, L, dtype=np.uint64).tobytes())
+    (tmp_path / "db.bin").write_bytes(db.tobytes())
+    (tmp_path / "query.bin").write_bytes(r["query"].tobytes())
+    (tmp_path / "key.bin").write_bytes(ref.ref_key(N, m, 77).tobytes())
+    out = subprocess.run([str(pir_exe), "run", str(tmp_path)], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert np.array_equal(np.frombuffer((tmp_path / "reply.bin").read_bytes(), dtype=np.uint64), r["reply"])
+    plain = np.frombuffer((tmp_path / "plain.bin").read_bytes(), dtype=np.uint8)
+    assert np.array_equal(plain[:alpha * L], db[chosen * alpha * L:(chosen + 1) * alpha * L])

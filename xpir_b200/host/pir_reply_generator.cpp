@@ -8,6 +8,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <iostream>
 #include <sstream>
 
@@ -231,6 +232,66 @@ bool PIRReplyGenerator::popReply(char **reply) {
   memcpy(out, (const char *)replies_.data() + next_reply_ * ct, ct);
   next_reply_++;
   *reply = out;
+  return true;
+}
+
+// ---- reply extraction ------------------------------------------------------------------
+
+PIRReplyExtraction::PIRReplyExtraction(PIRParameters &param, HomomorphicCrypto &cryptoMethod,
+                                       std::vector<uint64_t> secret_key, int device)
+    : param_(param), crypto_(cryptoMethod), key_(std::move(secret_key)) {
+  if ((uint64_t)key_.size() != (uint64_t)crypto_.getnbModuli() * crypto_.getpolyDegree())
+    throw Error(XPIR_B200_ERR_ARG, "PIRReplyExtraction: the key needs nb_moduli * poly_degree words");
+  xpir_b200_ctx *ctx = nullptr;
+  check(xpir_b200_ctx_create(&ctx, device, crypto_.getpolyDegree(), crypto_.getnbModuli()),
+        "PIRReplyExtraction: context");
+  ctx_.reset(ctx, [](xpir_b200_ctx *c) { xpir_b200_ctx_destroy(c); });
+}
+
+PIRReplyExtraction::~PIRReplyExtraction() {
+  for (char *r : replies_) free(r);
+}
+
+void PIRReplyExtraction::pushEncryptedReply(char *rawBytes) {
+  if (!rawBytes) throw Error(XPIR_B200_ERR_ARG, "pushEncryptedReply: null reply");
+  replies_.push_back(rawBytes);
+}
+
+uint64_t PIRReplyExtraction::getPlaintextReplyBytesize() const {
+  return (uint64_t)crypto_.getAbsBitPerCiphertext() * crypto_.getpolyDegree() / 8;
+}
+
+uint64_t PIRReplyExtraction::getnbPlaintextReplies(uint64_t maxFileBytesize) const {
+  // libpir.cpp:196-198
+  return (uint64_t)std::ceil((float)maxFileBytesize * param_.alpha / (float)getPlaintextReplyBytesize());
+}
+
+void PIRReplyExtraction::extractReply(uint64_t maxFileBytesize) {
+  if (crypto_.getAbsBitPerCiphertext() == 0) crypto_.setandgetAbsBitPerCiphertext(param_.n[0]);
+  const uint64_t agg = maxFileBytesize * param_.alpha, ct = crypto_.getCiphertextBytesize();
+  const uint32_t b = crypto_.getAbsBitPerCiphertext();
+  const uint64_t need = xpir_b200_extract_count(agg, param_.d, b, crypto_.getpolyDegree(), crypto_.getnbModuli());
+  if (replies_.size() < need) throw Error(XPIR_B200_ERR_STATE, "extractReply: fewer replies than the element needs");
+  std::vector<char> replies(need * ct);
+  for (uint64_t i = 0; i < need; i++) memcpy(replies.data() + i * ct, replies_[i], ct);
+  chunks_ = getnbPlaintextReplies(maxFileBytesize);
+  plain_.assign(chunks_ * getPlaintextReplyBytesize(), 0);
+  check(xpir_b200_extract(ctx_.get(), key_.data(), param_.d, b, agg, replies.data(), need, 0, plain_.data(),
+                          plain_.size(), 0),
+        "extractReply");
+  next_ = 0;
+  for (char *r : replies_) free(r);
+  replies_.clear();
+}
+
+bool PIRReplyExtraction::popPlaintextResult(char **result) {
+  if (!result || next_ >= chunks_) return false;
+  const uint64_t pb = getPlaintextReplyBytesize();
+  char *out = (char *)malloc(pb);
+  if (!out) throw Error(XPIR_B200_ERR_NOMEM, "popPlaintextResult");
+  memcpy(out, plain_.data() + next_ * pb, pb);
+  next_++;
+  *result = out;
   return true;
 }
 
