@@ -75,6 +75,13 @@ def lib():
                                        ctypes.c_uint32]
         L.xo_extract.argtypes = [_u64p, ctypes.c_uint64, _u64p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                  ctypes.c_uint32, ctypes.c_uint64, _u8p]
+        L.xo_salsa20_stream.argtypes = [_u8p, ctypes.c_uint64, ctypes.c_uint64, _u8p]
+        L.xo_keygen.argtypes = [_u8p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, _u64p]
+        L.xo_encrypt.argtypes = [_u8p, ctypes.c_uint64, _u64p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                 ctypes.c_uint32, ctypes.c_uint32, _u64p]
+        L.xo_query.argtypes = [_u8p, ctypes.c_uint64, _u64p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
+                               ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                               _u64p]
         L.xo_reply_count.restype = ctypes.c_uint64
         L.xo_reply_count.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                      ctypes.c_uint32, ctypes.c_uint32]
@@ -214,6 +221,48 @@ def extract(replies: np.ndarray, sk: np.ndarray, d: int, b: int, N: int, m: int,
     r = np.ascontiguousarray(replies, dtype=np.uint64)
     k = np.ascontiguousarray(sk, dtype=np.uint64)
     assert lib().xo_extract(_p64(r), r.size // (2 * m * N), _p64(k), d, b, N, m, agg_bytes, _p8(out)) == 0
+    return out
+
+
+def seeded_prng_key(seed: int) -> np.ndarray:
+    """The 32-byte Salsa20 key the reference's fastrandombytes draws from randombytes on its
+    first call, when randombytes is the seeded one linked into oracle/_ref
+    (oracle/ref/seeded_randombytes.cpp: splitmix64 from seed*0x2545F4914F6CDD1D + golden)."""
+    mask = (1 << 64) - 1
+    state = (seed * 0x2545F4914F6CDD1D + 0x9E3779B97F4A7C15) & mask
+    out = bytearray()
+    for _ in range(4):
+        state = (state + 0x9E3779B97F4A7C15) & mask
+        z = state
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & mask
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & mask
+        z ^= z >> 31
+        out += z.to_bytes(8, "little")
+    return np.frombuffer(bytes(out), dtype=np.uint8).copy()
+
+
+def salsa20_stream(key: np.ndarray, nonce: int, nbytes: int) -> np.ndarray:
+    out = np.zeros(nbytes, dtype=np.uint8)
+    k = np.ascontiguousarray(key, dtype=np.uint8)
+    lib().xo_salsa20_stream(_p8(out), nbytes, nonce, _p8(k))
+    return out
+
+
+def keygen(key: np.ndarray, nonce: int, N: int, m: int) -> np.ndarray:
+    out = np.zeros(m * N, dtype=np.uint64)
+    k = np.ascontiguousarray(key, dtype=np.uint8)
+    assert lib().xo_keygen(_p8(k), nonce, N, m, _p64(out)) == 0
+    return out
+
+
+def query(key: np.ndarray, first_nonce: int, sk: np.ndarray, n: list[int], chosen: int, b: int, N: int, m: int,
+          k: int = 80) -> np.ndarray:
+    """The sum(n) query ciphertexts for `chosen` (PIRQueryGenerator)."""
+    out = np.zeros(sum(n) * 2 * m * N, dtype=np.uint64)
+    kk = np.ascontiguousarray(key, dtype=np.uint8)
+    s = np.ascontiguousarray(sk, dtype=np.uint64)
+    narr = (ctypes.c_uint32 * len(n))(*n)
+    assert lib().xo_query(_p8(kk), first_nonce, _p64(s), len(n), narr, chosen, b, k, N, m, _p64(out)) == 0
     return out
 
 

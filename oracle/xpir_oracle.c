@@ -648,3 +648,145 @@ int xo_extract(const uint64_t *replies, uint64_t nb_replies, const uint64_t *sk,
   free(in);
   return 0;
 }
+
+/* ---- client-side query generation --------------------------------------------------- */
+
+/* Salsa20/20 keystream (the published algorithm; the reference calls NaCl's
+ * crypto_stream_salsa20 through fastrandombytes, crypto/prng/fastrandombytes.cpp:34-55):
+ * 64-byte blocks of the state (constants, 256-bit key, 64-bit nonce, 64-bit block counter
+ * from 0) after 20 rounds plus the input, little-endian. */
+#define XO_ROTL(v, c) (((v) << (c)) | ((v) >> (32 - (c))))
+static void salsa20_block(const uint32_t in[16], uint8_t out[64]) {
+  uint32_t x[16];
+  memcpy(x, in, sizeof(x));
+  for (int r = 0; r < 10; r++) {
+    x[4] ^= XO_ROTL(x[0] + x[12], 7);   x[8] ^= XO_ROTL(x[4] + x[0], 9);
+    x[12] ^= XO_ROTL(x[8] + x[4], 13);  x[0] ^= XO_ROTL(x[12] + x[8], 18);
+    x[9] ^= XO_ROTL(x[5] + x[1], 7);    x[13] ^= XO_ROTL(x[9] + x[5], 9);
+    x[1] ^= XO_ROTL(x[13] + x[9], 13);  x[5] ^= XO_ROTL(x[1] + x[13], 18);
+    x[14] ^= XO_ROTL(x[10] + x[6], 7);  x[2] ^= XO_ROTL(x[14] + x[10], 9);
+    x[6] ^= XO_ROTL(x[2] + x[14], 13);  x[10] ^= XO_ROTL(x[6] + x[2], 18);
+    x[3] ^= XO_ROTL(x[15] + x[11], 7);  x[7] ^= XO_ROTL(x[3] + x[15], 9);
+    x[11] ^= XO_ROTL(x[7] + x[3], 13);  x[15] ^= XO_ROTL(x[11] + x[7], 18);
+    x[1] ^= XO_ROTL(x[0] + x[3], 7);    x[2] ^= XO_ROTL(x[1] + x[0], 9);
+    x[3] ^= XO_ROTL(x[2] + x[1], 13);   x[0] ^= XO_ROTL(x[3] + x[2], 18);
+    x[6] ^= XO_ROTL(x[5] + x[4], 7);    x[7] ^= XO_ROTL(x[6] + x[5], 9);
+    x[4] ^= XO_ROTL(x[7] + x[6], 13);   x[5] ^= XO_ROTL(x[4] + x[7], 18);
+    x[11] ^= XO_ROTL(x[10] + x[9], 7);  x[8] ^= XO_ROTL(x[11] + x[10], 9);
+    x[9] ^= XO_ROTL(x[8] + x[11], 13);  x[10] ^= XO_ROTL(x[9] + x[8], 18);
+    x[12] ^= XO_ROTL(x[15] + x[14], 7); x[13] ^= XO_ROTL(x[12] + x[15], 9);
+    x[14] ^= XO_ROTL(x[13] + x[12], 13); x[15] ^= XO_ROTL(x[14] + x[13], 18);
+  }
+  for (int i = 0; i < 16; i++) {
+    const uint32_t v = x[i] + in[i];
+    out[4 * i] = (uint8_t)v;
+    out[4 * i + 1] = (uint8_t)(v >> 8);
+    out[4 * i + 2] = (uint8_t)(v >> 16);
+    out[4 * i + 3] = (uint8_t)(v >> 24);
+  }
+}
+
+static uint32_t le32(const uint8_t *b) { return (uint32_t)b[0] | (uint32_t)b[1] << 8 | (uint32_t)b[2] << 16 | (uint32_t)b[3] << 24; }
+
+void xo_salsa20_stream(uint8_t *out, uint64_t len, uint64_t nonce, const uint8_t key[32]) {
+  uint32_t in[16];
+  in[0] = 0x61707865u; in[5] = 0x3320646eu; in[10] = 0x79622d32u; in[15] = 0x6b206574u;  /* "expand 32-byte k" */
+  for (int i = 0; i < 4; i++) {
+    in[1 + i] = le32(key + 4 * i);
+    in[11 + i] = le32(key + 16 + 4 * i);
+  }
+  in[6] = (uint32_t)nonce;
+  in[7] = (uint32_t)(nonce >> 32);
+  uint8_t block[64];
+  for (uint64_t ctr = 0, off = 0; off < len; ctr++, off += 64) {
+    in[8] = (uint32_t)ctr;
+    in[9] = (uint32_t)(ctr >> 32);
+    salsa20_block(in, block);
+    memcpy(out + off, block, len - off < 64 ? (size_t)(len - off) : 64);
+  }
+}
+
+/* mask = 2^ceil(log2(bound)) - 1 with the reference's double arithmetic (NFLlib.cpp:305,339) */
+static uint64_t bound_mask(uint64_t bound) { return (1ULL << (unsigned int)ceil(log2((double)bound))) - 1; }
+
+/* NFLlib::setBoundedRandomPoly in uniform mode (crypto/NFLlib.cpp:325-353): one
+ * fastrandombytes call of m*N words (nonce `nonce`), masked and reduced per modulus. */
+static void uniform_poly(const uint8_t key[32], uint64_t nonce, uint32_t N, uint32_t m, uint64_t *out) {
+  xo_salsa20_stream((uint8_t *)out, (uint64_t)m * N * 8, nonce, key);
+  for (uint32_t c = 0; c < m; c++) {
+    const uint64_t p = xo_modulus(c), mask = bound_mask(p);
+    for (uint32_t i = 0; i < N; i++) {
+      uint64_t r = out[(uint64_t)c * N + i] & mask;
+      if (r >= p) r -= p;
+      out[(uint64_t)c * N + i] = r;
+    }
+  }
+}
+
+/* NFLLWE's secret key (crypto/NFLLWE.cpp:108-116): a uniform poly from the PRNG call with
+ * the given nonce (the first call, nonce 0, for a fresh crypto object). */
+int xo_keygen(const uint8_t key[32], uint64_t nonce, uint32_t N, uint32_t m, uint64_t *sk) {
+  if (!valid_shape(N, m)) return -1;
+  uniform_poly(key, nonce, N, m, sk);
+  return 0;
+}
+
+/* NFLLWE::encrypt(ui) -> enc (crypto/NFLLWE.cpp:276-372, 481-498) with the PRNG calls at
+ * nonces `nonce` (the noise, N words, NFLlib.cpp:290-321) and nonce+1 (the uniform a):
+ * b = NTT_phi(e*2^b mod p + m) + a*s, with e in [0, 2*(5k/2)-1) and m = ui on the
+ * constant coefficient of every modulus. */
+int xo_encrypt(const uint8_t key[32], uint64_t nonce, const uint64_t *sk, uint32_t ui, uint32_t b, uint32_t k,
+               uint32_t N, uint32_t m, uint64_t *ct) {
+  if (!valid_shape(N, m)) return -1;
+  uint64_t *a = ct, *bb = ct + (uint64_t)m * N;
+  const uint64_t ub = 2 * (5 * (uint64_t)k / 2) - 1, nmask = bound_mask(ub);
+  uint64_t *noise = (uint64_t *)malloc((size_t)N * 8);
+  if (!noise) return -2;
+  xo_salsa20_stream((uint8_t *)noise, (uint64_t)N * 8, nonce, key);
+  for (uint32_t i = 0; i < N; i++) {
+    noise[i] &= nmask;
+    if (noise[i] >= ub) noise[i] -= ub;
+  }
+  for (uint32_t c = 0; c < m; c++) {
+    const uint64_t p = xo_modulus(c);
+    const uint64_t amp = (uint64_t)(((u128)1 << b) % p);  /* 2^b mod p (b < 128) */
+    const uint64_t amps = shoup(amp, p);
+    for (uint32_t i = 0; i < N; i++) {
+      uint64_t v = mulmod_shoup(noise[i], amp, amps, p);
+      uint64_t z = v + (i == 0 ? ui : 0);
+      z -= (z >= p) ? p : 0;   /* addmod */
+      if (z > p) z -= p;
+      bb[(uint64_t)c * N + i] = z;
+    }
+  }
+  free(noise);
+  xo_ntt_phi(bb, 1, N, m);
+  uniform_poly(key, nonce + 1, N, m, a);
+  for (uint32_t c = 0; c < m; c++) {
+    const uint64_t p = xo_modulus(c);
+    /* with SHOUP defined (crypto/NFLLWE.hpp:21) both halves leave fully reduced
+     * (crypto/NFLLWE.cpp:355-358) */
+    for (uint64_t i = (uint64_t)c * N; i < (uint64_t)(c + 1) * N; i++) {
+      bb[i] = mac_shoup(bb[i], a[i], sk[i], shoup(sk[i], p), p) % p;
+      a[i] %= p;
+    }
+  }
+  return 0;
+}
+
+/* PIRQueryGenerator_internal::generateQuery (pir/queryGen/PIRQueryGenerator_internal.cpp:37-70):
+ * for level j, n[j] encryptions of [i == coord_j] where coord is the chosen element in
+ * mixed radix n[0], n[1], ...; ciphertext t uses nonces first_nonce + 2t and + 2t + 1. */
+int xo_query(const uint8_t key[32], uint64_t first_nonce, const uint64_t *sk, uint32_t d, const uint32_t *n,
+             uint64_t chosen, uint32_t b, uint32_t k, uint32_t N, uint32_t m, uint64_t *out) {
+  uint64_t t = 0, x = chosen;
+  const uint64_t ct_words = 2ull * m * N;
+  for (uint32_t j = 0; j < d; j++) {
+    const uint64_t coord = x % n[j];
+    x /= n[j];
+    for (uint64_t i = 0; i < n[j]; i++, t++)
+      if (xo_encrypt(key, first_nonce + 2 * t, sk, i == coord ? 1u : 0u, b, k, N, m, out + t * ct_words) != 0)
+        return -1;
+  }
+  return 0;
+}

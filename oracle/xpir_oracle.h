@@ -115,6 +115,19 @@ uint64_t xo_extract_count(uint64_t agg_bytes, uint32_t lvl, uint32_t b, uint32_t
 int xo_extract(const uint64_t *replies, uint64_t nb_replies, const uint64_t *sk, uint32_t d, uint32_t b, uint32_t N,
                uint32_t m, uint64_t agg_bytes, uint8_t *out);
 
+/* Client-side query generation.  Salsa20/20 keystream for one fastrandombytes call
+ * (crypto/prng/fastrandombytes.cpp:34-55): len bytes, 64-bit nonce, 32-byte key. */
+void xo_salsa20_stream(uint8_t *out, uint64_t len, uint64_t nonce, const uint8_t key[32]);
+/* NFLLWE's secret key from the PRNG call with the given nonce (crypto/NFLLWE.cpp:108-116). */
+int xo_keygen(const uint8_t key[32], uint64_t nonce, uint32_t N, uint32_t m, uint64_t *sk);
+/* NFLLWE::encrypt(ui) with the noise at nonce and the uniform a at nonce+1
+ * (crypto/NFLLWE.cpp:276-372, 481-498). */
+int xo_encrypt(const uint8_t key[32], uint64_t nonce, const uint64_t *sk, uint32_t ui, uint32_t b, uint32_t k,
+               uint32_t N, uint32_t m, uint64_t *ct);
+/* The sum(n) query ciphertexts for the chosen element (PIRQueryGenerator_internal.cpp:37-70). */
+int xo_query(const uint8_t key[32], uint64_t first_nonce, const uint64_t *sk, uint32_t d, const uint32_t *n,
+             uint64_t chosen, uint32_t b, uint32_t k, uint32_t N, uint32_t m, uint64_t *out);
+
 #ifdef __cplusplus
 }
 #endif

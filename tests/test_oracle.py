@@ -155,3 +155,24 @@ def test_extraction_round_trip_with_reference_key(ref):
     got = ref.extract(r["reply"], key, len(n), b, N, m, L * alpha)
     assert np.array_equal(got, db[chosen * alpha * L:(chosen + 1) * alpha * L])
     assert np.array_equal(got, r["plain"])
+
+
+@pytest.mark.parametrize("N,m", [(1024, 1), (2048, 2), (4096, 3)])
+def test_keygen_matches_reference(ref, N, m):
+    """The Salsa20 keystream restatement keyed like the reference's fastrandombytes gives
+    the reference's secret key (the first PRNG call of a fresh crypto object)."""
+    key = ref.seeded_prng_key(9)
+    assert np.array_equal(ref.keygen(key, 0, N, m), ref.ref_key(N, m, 9))
+
+
+@pytest.mark.parametrize("N,m,n,alpha,F,L,chosen,seed", [
+    (1024, 2, [5, 4], 1, 20, 300, 13, 21), (2048, 3, [7], 2, 13, 900, 5, 4), (512, 1, [3, 3, 2], 1, 18, 200, 11, 8)])
+def test_query_generation_matches_reference(ref, N, m, n, alpha, F, L, chosen, seed):
+    """Query ciphertexts from the restatement (noise, amplification, NTT, uniform a, a*s,
+    full reduction) equal the reference's PIRQueryGenerator output word for word."""
+    db = np.random.default_rng(1).integers(0, 256, size=F * L, dtype=np.uint8)
+    r = ref.ref_run(N, m, n, alpha, db, F, L, keyseed=seed, chosen=chosen, extract=False)
+    key = ref.seeded_prng_key(seed)
+    sk = ref.keygen(key, 0, N, m)
+    b = ref.bits_per_coeff(N, m, n[0])
+    assert np.array_equal(ref.query(key, 1, sk, n, chosen, b, N, m), r["query"])
