@@ -172,6 +172,22 @@ XPIR_B200_API int xpir_b200_extract(xpir_b200_ctx *ctx, const uint64_t *secret_k
                                     int replies_on_device, void *plaintext, uint64_t capacity_bytes,
                                     int out_on_device);
 
+/* ---- query generation (client side) ------------------------------------------------ */
+/* The sum(n) query ciphertexts of PIRQueryGenerator::generateQuery for chosen_element
+ * (pir/queryGen/PIRQueryGenerator_internal.cpp:37-85), on the GPU: NFLLWE::encrypt of 1 at
+ * each level's coordinate and of 0 elsewhere (crypto/NFLLWE.cpp:276-372, 481-498).  The
+ * randomness is the reference's fastrandombytes stream (crypto/prng/fastrandombytes.cpp:34-55):
+ * Salsa20/20 under the client's 32-byte prng_key, one nonce per PRNG call; ciphertext t
+ * draws its noise with nonce first_nonce + 2t and its uniform half with first_nonce + 2t + 1
+ * (for a fresh crypto object, key generation used nonce 0, so first_nonce = 1).
+ * secret_key: host, [nb_moduli][poly_degree] words as NFLLWE's secretKey.  query receives
+ * the ciphertexts back to back (host memory unless out_on_device).  No counterpart on the
+ * reference's server path: the reference generates queries on the client's CPU. */
+XPIR_B200_API int xpir_b200_generate_query(xpir_b200_ctx *ctx, const uint8_t *prng_key, uint64_t first_nonce,
+                                           const uint64_t *secret_key, uint32_t d, const uint32_t *n,
+                                           uint64_t chosen_element, uint32_t bits_per_coeff, uint32_t security_bits,
+                                           void *query, uint64_t capacity_bytes, int out_on_device);
+
 /* ---- serving loop ------------------------------------------------------------------ */
 /* A server over one or more contexts (one lane each: a worker thread and the context's
  * stream, so lanes run concurrently on the GPU).  Queries wait in FIFO order per lane

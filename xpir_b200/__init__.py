@@ -90,6 +90,8 @@ def _load():
         L.xpir_b200_extract_count.argtypes = [c_u64, c_u32, c_u32, c_u32, c_u32]
         L.xpir_b200_extract.argtypes = [vp, vp, c_u32, c_u32, c_u64, vp, c_u64, ctypes.c_int, vp, c_u64,
                                         ctypes.c_int]
+        L.xpir_b200_generate_query.argtypes = [vp, vp, c_u64, vp, c_u32, ctypes.POINTER(c_u32), c_u64, c_u32,
+                                                c_u32, vp, c_u64, ctypes.c_int]
         L.xpir_b200_server_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), c_u32, c_u64, c_u32]
         L.xpir_b200_server_submit.argtypes = [vp, vp, c_u32, ctypes.POINTER(c_u32), vp, vp, c_u64,
                                               ctypes.POINTER(c_u64)]
@@ -280,6 +282,21 @@ class Context:
         nrep //= 16 * self.m * self.N
         _check(_load().xpir_b200_extract(self.handle, sk.ctypes.data, d, b, aggregated_bytes, _ptr(replies), nrep,
                                          _on_device(replies), _ptr(out), cap, _on_device(out)), "extract")
+        return out
+
+    def generate_query(self, prng_key: np.ndarray, first_nonce: int, secret_key: np.ndarray, n: list[int],
+                       chosen: int, b: int, security_bits: int = 80, out=None):
+        """Client-side query generation on the GPU (PIRQueryGenerator with the reference's
+        Salsa20 PRNG stream): sum(n) ciphertexts for element `chosen`."""
+        key = np.ascontiguousarray(prng_key, dtype=np.uint8)
+        sk = np.ascontiguousarray(secret_key, dtype=np.uint64)
+        if out is None:
+            out = np.zeros(sum(n) * self.ct_words, dtype=np.uint64)
+        cap = out.nbytes if isinstance(out, np.ndarray) else out.numel() * out.element_size()
+        narr = (ctypes.c_uint32 * len(n))(*n)
+        _check(_load().xpir_b200_generate_query(self.handle, key.ctypes.data, first_nonce, sk.ctypes.data, len(n),
+                                                narr, chosen, b, security_bits, _ptr(out), cap, _on_device(out)),
+               "generate_query")
         return out
 
     def autotune(self, db: Database, n: list[int], query) -> int:

@@ -19,7 +19,7 @@ CSRC = PKG / "csrc"
 LIB = PKG / "libxpir_b200.so"
 PIR_LIB = PKG / "libxpir_b200_pir.so"  # the libpir-shaped C++ API (host code over the C ABI)
 PIR_SOURCES = ["host/pir_reply_generator.cpp"]
-SOURCES = ["params.cpp", "sm100_host.cu", "import.cu", "reply.cu", "capi.cu", "batch.cu", "server.cu", "extract.cu", "noalloc.cu"]
+SOURCES = ["params.cpp", "sm100_host.cu", "import.cu", "reply.cu", "capi.cu", "batch.cu", "server.cu", "extract.cu", "querygen.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
