@@ -188,6 +188,12 @@ XPIR_B200_API int xpir_b200_generate_query(xpir_b200_ctx *ctx, const uint8_t *pr
                                            uint64_t chosen_element, uint32_t bits_per_coeff, uint32_t security_bits,
                                            void *query, uint64_t capacity_bytes, int out_on_device);
 
+/* NFLLWE's secret key (crypto/NFLLWE.cpp:108-116): the uniform polynomial of the PRNG
+ * call with the given nonce (0 for a fresh crypto object), written to host memory
+ * ([nb_moduli][poly_degree] words, NTT domain). */
+XPIR_B200_API int xpir_b200_generate_secret_key(xpir_b200_ctx *ctx, const uint8_t *prng_key, uint64_t nonce,
+                                                uint64_t *secret_key);
+
 /* ---- serving loop ------------------------------------------------------------------ */
 /* A server over one or more contexts (one lane each: a worker thread and the context's
  * stream, so lanes run concurrently on the GPU).  Queries wait in FIFO order per lane

@@ -36,15 +36,22 @@ def test_query_matches_reference(engine, ref):
         assert np.array_equal(ctx.generate_query(key, 1, ref.ref_key(N, m, seed), n, chosen, b), r["query"])
 
 
+@pytest.mark.parametrize("N,m", [(1024, 1), (2048, 2), (4096, 3)])
+def test_secret_key_matches_oracle(engine, oracle, N, m):
+    key = oracle.seeded_prng_key(12)
+    with engine.Context(N, m) as ctx:
+        assert np.array_equal(ctx.generate_secret_key(key, 0), oracle.keygen(key, 0, N, m))
+
+
 def test_gpu_only_round_trip(engine, oracle):
-    """Key (restated keygen), query, import, reply and extraction: only the key is made on
-    the CPU; the chosen aggregated element comes back."""
+    """Key, query, import, reply and extraction all on the GPU: the chosen aggregated
+    element comes back."""
     N, m, n, alpha, F, L, chosen = 2048, 2, [9, 8], 3, 200, 1000, 41
     db = np.random.default_rng(4).integers(0, 256, size=F * L, dtype=np.uint8)
     key = oracle.seeded_prng_key(77)
-    sk = oracle.keygen(key, 0, N, m)
     b = engine.bits_per_coeff(N, m, n[0])
     with engine.Context(N, m) as ctx:
+        sk = ctx.generate_secret_key(key, 0)
         q = ctx.generate_query(key, 1, sk, n, chosen, b)
         dbh = ctx.import_db(db, F, L, alpha, b)
         reply = ctx.reply(dbh, n, q)

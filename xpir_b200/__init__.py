@@ -92,6 +92,7 @@ def _load():
                                         ctypes.c_int]
         L.xpir_b200_generate_query.argtypes = [vp, vp, c_u64, vp, c_u32, ctypes.POINTER(c_u32), c_u64, c_u32,
                                                 c_u32, vp, c_u64, ctypes.c_int]
+        L.xpir_b200_generate_secret_key.argtypes = [vp, vp, c_u64, vp]
         L.xpir_b200_server_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), c_u32, c_u64, c_u32]
         L.xpir_b200_server_submit.argtypes = [vp, vp, c_u32, ctypes.POINTER(c_u32), vp, vp, c_u64,
                                               ctypes.POINTER(c_u64)]
@@ -282,6 +283,14 @@ class Context:
         nrep //= 16 * self.m * self.N
         _check(_load().xpir_b200_extract(self.handle, sk.ctypes.data, d, b, aggregated_bytes, _ptr(replies), nrep,
                                          _on_device(replies), _ptr(out), cap, _on_device(out)), "extract")
+        return out
+
+    def generate_secret_key(self, prng_key: np.ndarray, nonce: int = 0) -> np.ndarray:
+        """NFLLWE key generation on the GPU from the PRNG call with `nonce`."""
+        key = np.ascontiguousarray(prng_key, dtype=np.uint8)
+        out = np.zeros(self.m * self.N, dtype=np.uint64)
+        _check(_load().xpir_b200_generate_secret_key(self.handle, key.ctypes.data, nonce, out.ctypes.data),
+               "generate_secret_key")
         return out
 
     def generate_query(self, prng_key: np.ndarray, first_nonce: int, secret_key: np.ndarray, n: list[int],

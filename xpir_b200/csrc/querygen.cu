@@ -133,6 +133,23 @@ __global__ void __launch_bounds__(256) encrypt_kernel(const QueryGenArgs g, cons
   }
 }
 
+// NFLLWE's secret key (crypto/NFLLWE.cpp:108-116): the uniform poly of one PRNG call.
+__global__ void __launch_bounds__(256) keygen_kernel(const QueryGenArgs g, uint64_t nonce, uint32_t N,
+                                                     const DevModuli dm, uint64_t *__restrict__ sk) {
+  const uint32_t c = blockIdx.y;
+  const uint64_t p = dm.p[c];
+  for (uint32_t blk = blockIdx.x * blockDim.x + threadIdx.x; blk < N / 8; blk += gridDim.x * blockDim.x) {
+    uint32_t w[16];
+    salsa20_block(g.key, nonce, (uint64_t)c * (N / 8) + blk, w);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      uint64_t a = ((uint64_t)w[2 * k] | (uint64_t)w[2 * k + 1] << 32) & g.uniform_mask[c];
+      if (a >= p) a -= p;
+      sk[(uint64_t)c * N + blk * 8 + k] = a;
+    }
+  }
+}
+
 int status_of(cudaError_t e) {
   if (e == cudaSuccess) return XPIR_B200_OK;
   (void)cudaGetLastError();
@@ -218,6 +235,36 @@ extern "C" int xpir_b200_generate_query(xpir_b200_ctx *ctx, const uint8_t *prng_
   cudaFreeAsync(d_sk, st);
   cudaFreeAsync(d_sks, st);
   if (d_out) cudaFreeAsync(d_out, st);
+  const cudaError_t se = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = se;
+  return status_of(e);
+}
+
+extern "C" int xpir_b200_generate_secret_key(xpir_b200_ctx *ctx, const uint8_t *prng_key, uint64_t nonce,
+                                             uint64_t *secret_key) {
+  if (!ctx || !prng_key || !secret_key) return XPIR_B200_ERR_ARG;
+  const ParamSet &ps = ctx->ps;
+  const uint64_t mN = (uint64_t)ps.m * ps.N;
+  QueryGenArgs g;
+  memset(&g, 0, sizeof(g));
+  for (int i = 0; i < 8; i++)
+    g.key[i] = (uint32_t)prng_key[4 * i] | (uint32_t)prng_key[4 * i + 1] << 8 | (uint32_t)prng_key[4 * i + 2] << 16 |
+               (uint32_t)prng_key[4 * i + 3] << 24;
+  for (uint32_t c = 0; c < ps.m; c++) g.uniform_mask[c] = bound_mask(ps.mod[c].p);
+  const DevModuli dm = make_dev_moduli(ps);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return status_of(e);
+  cudaStream_t st = ctx->stream;
+  uint64_t *d_sk = nullptr;
+  e = cudaMallocAsync((void **)&d_sk, mN * 8, st);
+  if (e == cudaSuccess) {
+    keygen_kernel<<<dim3((ps.N / 8 + 255) / 256, ps.m), 256, 0, st>>>(g, nonce, ps.N, dm, d_sk);
+    e = cudaGetLastError();
+    ctx->launches++;
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(secret_key, d_sk, mN * 8, cudaMemcpyDeviceToHost, st);
+  if (d_sk) cudaFreeAsync(d_sk, st);
   const cudaError_t se = cudaStreamSynchronize(st);
   if (e == cudaSuccess) e = se;
   return status_of(e);
