@@ -195,13 +195,15 @@ XPIR_B200_API int xpir_b200_generate_secret_key(xpir_b200_ctx *ctx, const uint8_
                                                 uint64_t *secret_key);
 
 /* ---- serving loop ------------------------------------------------------------------ */
-/* A server over one or more contexts (one lane each: a worker thread and the context's
- * stream, so lanes run concurrently on the GPU).  Queries wait in FIFO order per lane
- * and are admitted while their device footprint (query, replies, recursion workspace)
- * fits what is left of `device_budget_bytes`; each lane runs the admitted prefix (at
- * most max_batch queries) as one xpir_b200_reply_batch, and queries that arrive
- * meanwhile join the next batch.  No counterpart in the reference, whose server handles
- * one query per session (apps/server/PIRSession.cpp:45-111, 467-565). */
+/* A server over one or more contexts, one lane each.  Queries wait in FIFO order per
+ * lane and are admitted while their device footprint (query, replies, recursion
+ * workspace) fits what is left of `device_budget_bytes`; each lane runs the admitted
+ * prefix (at most max_batch queries) as one xpir_b200_reply_batch, and queries that arrive
+ * meanwhile join the next batch.  A lane is a two-stage pipeline (an uploading thread with
+ * its own copy stream, a computing thread with the context's stream), so one batch's
+ * host-to-device copies overlap the previous batch's replies, and lanes overlap each other.
+ * No counterpart in the reference, whose server handles one query per session
+ * (apps/server/PIRSession.cpp:45-111, 467-565). */
 typedef struct xpir_b200_server xpir_b200_server;
 XPIR_B200_API int xpir_b200_server_create(xpir_b200_server **srv, xpir_b200_ctx *const *ctxs, uint32_t nctx,
                                           uint64_t device_budget_bytes, uint32_t max_batch);

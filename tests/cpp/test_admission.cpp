@@ -6,7 +6,10 @@
 //   4. jobs that arrive while a batch runs are admitted together in a later batch
 //      (continuous batching), never more than max_batch at a time;
 //   5. lanes run concurrently (two lanes' batches overlap in time);
-//   6. a head-of-line job that does not fit waits for memory rather than being skipped.
+//   6. a head-of-line job that does not fit waits for memory rather than being skipped;
+//   7. as a two-stage pipeline (depth 2), stage 1 of a lane's next batch overlaps stage 2
+//      of its current one, at most two batches per lane are in flight, stage 2 sees the
+//      batches in admission order, and every job completes.
 #include <stdio.h>
 
 #include <atomic>
@@ -132,6 +135,54 @@ int main() {
   adm.release(slow);
   adm.stop();
   CHECK(adm.submit(0, 1, nullptr) == 0);  // stopped: refused
-  printf("ok %llu batches\n", (unsigned long long)adm.stats().batches);
+  const unsigned long long plain_batches = adm.stats().batches;
+
+  // 7. Two-stage pipeline.
+  {
+    std::mutex mu;
+    std::atomic<int> inflight[2] = {{0}, {0}}, max_inflight{0}, overlaps{0};
+    std::atomic<int> in_stage2[2] = {{0}, {0}};
+    std::vector<uint64_t> order[2];
+    Admission pipe(
+        2, budget, 3,
+        [&](uint32_t lane, std::vector<Job *> &batch) {
+          const int f = ++inflight[lane];
+          int mx = max_inflight.load();
+          while (f > mx && !max_inflight.compare_exchange_weak(mx, f)) {
+          }
+          if (in_stage2[lane].load()) overlaps++;
+          std::this_thread::sleep_for(std::chrono::milliseconds(8));
+          for (Job *j : batch) j->status = 1;  // stage 1 done
+        },
+        [&](uint32_t lane, std::vector<Job *> &batch) {
+          in_stage2[lane] = 1;
+          std::this_thread::sleep_for(std::chrono::milliseconds(20));
+          {
+            std::lock_guard<std::mutex> lk(mu);
+            for (Job *j : batch) order[lane].push_back(j->ticket);
+          }
+          for (Job *j : batch) j->status = j->status == 1 ? 2 : -1;
+          in_stage2[lane] = 0;
+          --inflight[lane];
+        },
+        2);
+    std::vector<uint64_t> t2[2];
+    for (int i = 0; i < 30; i++) {
+      for (uint32_t lane = 0; lane < 2; lane++) t2[lane].push_back(pipe.submit(lane, 50 + 13 * (i % 4), nullptr));
+      std::this_thread::sleep_for(std::chrono::milliseconds(3));
+    }
+    for (uint32_t lane = 0; lane < 2; lane++)
+      for (uint64_t t : t2[lane]) {
+        Job *j = pipe.wait(t, 20000);
+        CHECK(j && j->status == 2);
+        pipe.release(t);
+      }
+    CHECK(max_inflight.load() <= 2);
+    CHECK(overlaps.load() > 0);
+    CHECK(pipe.stats().completed == 60 && pipe.stats().peak_in_use <= budget);
+    for (int lane = 0; lane < 2; lane++) CHECK(order[lane] == t2[lane]);
+    pipe.stop();
+  }
+  printf("ok %llu batches\n", plain_batches);
   return 0;
 }

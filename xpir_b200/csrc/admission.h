@@ -6,6 +6,11 @@
 // that arrive while a batch runs wait for the next one; a request larger than the whole
 // budget is refused at submission.  The executor (the GPU in the server, a fake in the
 // CPU tests) is a callback.
+//
+// With a second stage, a lane is a two-step pipeline: the admitting worker runs stage 1
+// (in the server: the host-to-device copies) and hands the batch to the lane's second
+// thread, which runs stage 2 (the replies and the copies back) and completes it; up to
+// `depth` batches per lane are in flight, so batch k+1's copies overlap batch k's work.
 #pragma once
 
 #include <stdint.h>
@@ -42,9 +47,19 @@ class Admission {
   // Runs one batch of jobs of one lane; sets each job's status.
   typedef std::function<void(uint32_t lane, std::vector<Job *> &batch)> Executor;
 
-  Admission(uint32_t lanes, uint64_t budget, uint32_t max_batch, Executor exec)
-      : budget_(budget), max_batch_(max_batch ? max_batch : 1), exec_(std::move(exec)), queues_(lanes) {
+  Admission(uint32_t lanes, uint64_t budget, uint32_t max_batch, Executor exec, Executor stage2 = nullptr,
+            uint32_t depth = 2)
+      : budget_(budget),
+        max_batch_(max_batch ? max_batch : 1),
+        depth_(stage2 ? (depth ? depth : 1) : 1),
+        exec_(std::move(exec)),
+        stage2_(std::move(stage2)),
+        queues_(lanes),
+        handoff_(lanes),
+        inflight_(lanes, 0) {
     for (uint32_t l = 0; l < lanes; l++) workers_.emplace_back([this, l] { run(l); });
+    if (stage2_)
+      for (uint32_t l = 0; l < lanes; l++) workers_.emplace_back([this, l] { run_stage2(l); });
   }
 
   ~Admission() { stop(); }
@@ -120,12 +135,13 @@ class Admission {
   void run(uint32_t lane) {
     std::unique_lock<std::mutex> lk(mu_);
     for (;;) {
-      // Admit the longest FIFO prefix that fits the remaining budget.
+      // Admit the longest FIFO prefix that fits the remaining budget, once the lane has
+      // room for another batch in flight.
       std::vector<Job *> batch;
       cv_.wait(lk, [&] {
         if (stopping_) return true;
         auto &q = queues_[lane];
-        return !q.empty() && q.front()->footprint <= budget_ - in_use_;
+        return inflight_[lane] < depth_ && !q.empty() && q.front()->footprint <= budget_ - in_use_;
       });
       if (stopping_) return;
       auto &q = queues_[lane];
@@ -137,29 +153,58 @@ class Admission {
         batch.push_back(j);
       }
       if (in_use_ > stats_.peak_in_use) stats_.peak_in_use = in_use_;
+      inflight_[lane]++;
       lk.unlock();
       exec_(lane, batch);
-      const double t = now();
       lk.lock();
-      for (Job *j : batch) {
-        in_use_ -= j->footprint;
-        j->t_done = t;
-        j->done = true;
+      if (stage2_) {
+        handoff_[lane].push_back(std::move(batch));
+        cv_.notify_all();
+      } else {
+        complete(lane, batch);
       }
-      stats_.batches++;
-      stats_.completed += batch.size();
-      if (batch.size() > stats_.max_batch_seen) stats_.max_batch_seen = batch.size();
-      done_cv_.notify_all();
-      cv_.notify_all();  // memory freed: other lanes may admit
     }
+  }
+
+  // Stage 2 of a pipelined lane: in admission order, and drained before stop returns.
+  void run_stage2(uint32_t lane) {
+    std::unique_lock<std::mutex> lk(mu_);
+    for (;;) {
+      cv_.wait(lk, [&] { return !handoff_[lane].empty() || (stopping_ && inflight_[lane] == 0); });
+      if (handoff_[lane].empty()) return;
+      std::vector<Job *> batch = std::move(handoff_[lane].front());
+      handoff_[lane].pop_front();
+      lk.unlock();
+      stage2_(lane, batch);
+      lk.lock();
+      complete(lane, batch);
+    }
+  }
+
+  // Called with mu_ held: releases the batch's memory and marks its jobs done.
+  void complete(uint32_t lane, std::vector<Job *> &batch) {
+    const double t = now();
+    for (Job *j : batch) {
+      in_use_ -= j->footprint;
+      j->t_done = t;
+      j->done = true;
+    }
+    inflight_[lane]--;
+    stats_.batches++;
+    stats_.completed += batch.size();
+    if (batch.size() > stats_.max_batch_seen) stats_.max_batch_seen = batch.size();
+    done_cv_.notify_all();
+    cv_.notify_all();  // memory and a pipeline slot freed: lanes may admit
   }
 
   std::mutex mu_;
   std::condition_variable cv_, done_cv_;
   const uint64_t budget_;
-  const uint32_t max_batch_;
-  Executor exec_;
+  const uint32_t max_batch_, depth_;
+  Executor exec_, stage2_;
   std::vector<std::deque<Job *>> queues_;
+  std::vector<std::deque<std::vector<Job *>>> handoff_;
+  std::vector<uint32_t> inflight_;
   std::map<uint64_t, std::unique_ptr<Job>> jobs_;
   std::vector<std::thread> workers_;
   uint64_t in_use_ = 0, next_ticket_ = 0;

@@ -1,6 +1,8 @@
 // Serving loop: continuous batching of queries over resident databases, admission by a
-// device-memory budget, one lane (worker thread + the context's stream) per context, so
-// that batches of different parameter sets overlap on the GPU.  See admission.h for the
+// device-memory budget, one lane per context (an uploading thread with its copy stream
+// and a computing thread with the context's stream), so that batches of different
+// parameter sets overlap on the GPU and, within a lane, one batch's copies overlap the
+// previous batch's replies.  See admission.h for the
 // queueing rules; this file runs a batch on the engine.
 //
 // No counterpart in the reference, whose server answers one query per session and
@@ -28,23 +30,56 @@ struct ServedQuery {
   const void *host_query = nullptr;  // caller's buffer, valid until the wait returns
   void *host_replies = nullptr;
   uint64_t query_bytes = 0, reply_bytes = 0, capacity = 0, nb_replies = 0;
+  // set by the upload stage, used by the compute stage
+  void *dq = nullptr, *dr = nullptr;
+  cudaEvent_t uploaded = nullptr;  // on the batch's first query only
+  int upload_status = 0;
 };
 
 }  // namespace
 
 struct xpir_b200_server {
   std::vector<xpir_b200_ctx *> ctxs;
-  std::vector<cudaMemPool_t> pools;  // one stream-ordered pool per lane, on its device
+  std::vector<cudaMemPool_t> pools;         // one stream-ordered pool per lane, on its device
+  std::vector<cudaStream_t> copy_streams;   // host-to-device copies, beside the context's stream
   std::unique_ptr<xpir::Admission> adm;
 };
 
 namespace {
 
-// Runs one admitted batch of one lane.  Every device buffer of the batch (queries,
-// replies, recursion workspace) comes from the lane's stream-ordered pool and goes back
-// to it in stream order, so the batch neither synchronises the device nor holds memory
-// beyond the footprints admission reserved for it; other lanes keep running meanwhile.
-void run_batch(xpir_b200_server *srv, uint32_t lane, std::vector<xpir::Job *> &batch) {
+int status_of_error(cudaError_t e) {
+  return e == cudaErrorMemoryAllocation ? XPIR_B200_ERR_NOMEM : XPIR_B200_ERR_CUDA;
+}
+
+// A lane is a two-stage pipeline (admission.h).  Every device buffer of a batch
+// (queries, replies, recursion workspace) comes from the lane's stream-ordered pool and
+// goes back to it in stream order, so no stage synchronises the device or holds memory
+// beyond the footprints admission reserved; other lanes keep running meanwhile.
+//
+// Stage 1, on the admitting thread: the batch's query and reply buffers and the queries'
+// host-to-device copies, on the lane's copy stream; an event marks their completion.
+void upload_batch(xpir_b200_server *srv, uint32_t lane, std::vector<xpir::Job *> &batch) {
+  xpir_b200_ctx *ctx = srv->ctxs[lane];
+  cudaStream_t cs = srv->copy_streams[lane];
+  cudaError_t e = cudaSetDevice(ctx->device);
+  for (size_t i = 0; i < batch.size(); i++) {
+    auto *q = (ServedQuery *)batch[i]->payload.get();
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&q->dq, q->query_bytes ? q->query_bytes : 256, srv->pools[lane], cs);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&q->dr, q->reply_bytes ? q->reply_bytes : 256, srv->pools[lane], cs);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(q->dq, q->host_query, q->query_bytes, cudaMemcpyHostToDevice, cs);
+  }
+  auto *q0 = (ServedQuery *)batch[0]->payload.get();
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&q0->uploaded, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventRecord(q0->uploaded, cs);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    for (auto *j : batch) ((ServedQuery *)j->payload.get())->upload_status = status_of_error(e);
+  }
+}
+
+// Stage 2, on the lane's second thread: once the copies are done, one batched reply on
+// the context's stream (workspace from the pool), the replies copied back, buffers freed.
+void compute_batch(xpir_b200_server *srv, uint32_t lane, std::vector<xpir::Job *> &batch) {
   xpir_b200_ctx *ctx = srv->ctxs[lane];
   cudaStream_t st = ctx->stream;
   cudaMemPool_t pool = srv->pools[lane];
@@ -55,22 +90,20 @@ void run_batch(xpir_b200_server *srv, uint32_t lane, std::vector<xpir::Job *> &b
     if (e == cudaSuccess) held.push_back(*p);
     return e;
   };
+  auto *q0 = (ServedQuery *)batch[0]->payload.get();
   cudaError_t e = cudaSetDevice(ctx->device);
+  const int upload = q0->upload_status;
+  if (e == cudaSuccess && upload == XPIR_B200_OK) e = cudaStreamWaitEvent(st, q0->uploaded, 0);
   std::vector<xpir_b200_request> reqs(batch.size());
-  std::vector<void *> dr(batch.size(), nullptr);
-  for (size_t i = 0; i < batch.size() && e == cudaSuccess; i++) {
+  for (size_t i = 0; i < batch.size(); i++) {
     auto *q = (ServedQuery *)batch[i]->payload.get();
-    void *dq = nullptr;
-    e = alloc(q->query_bytes, &dq);
-    if (e == cudaSuccess) e = alloc(q->reply_bytes, &dr[i]);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dq, q->host_query, q->query_bytes, cudaMemcpyHostToDevice, st);
     xpir_b200_request &r = reqs[i];
     memset(&r, 0, sizeof(r));
     r.db = q->db;
     r.d = q->d;
     memcpy(r.n, q->n, sizeof(r.n));
-    r.query = dq;
-    r.replies = dr[i];
+    r.query = q->dq;
+    r.replies = q->dr;
     r.capacity_bytes = q->reply_bytes;
   }
   const xpir::WorkspaceFn ws = [&](size_t a, size_t b, size_t f, void **pa, void **pb, void **pf) -> cudaError_t {
@@ -78,20 +111,29 @@ void run_batch(xpir_b200_server *srv, uint32_t lane, std::vector<xpir::Job *> &b
     if (r == cudaSuccess) r = alloc(b, pb);
     return r == cudaSuccess ? alloc(f, pf) : r;
   };
-  if (e == cudaSuccess) xpir::reply_batch_impl(ctx, reqs.data(), (uint32_t)reqs.size(), 0, &ws);
+  const bool run = e == cudaSuccess && upload == XPIR_B200_OK;
+  if (run) xpir::reply_batch_impl(ctx, reqs.data(), (uint32_t)reqs.size(), 0, &ws);
   for (size_t i = 0; i < batch.size(); i++) {
     auto *q = (ServedQuery *)batch[i]->payload.get();
-    int s = e == cudaSuccess ? reqs[i].status : (e == cudaErrorMemoryAllocation ? XPIR_B200_ERR_NOMEM : XPIR_B200_ERR_CUDA);
+    int s = run ? reqs[i].status : (upload != XPIR_B200_OK ? upload : status_of_error(e));
     if (s == XPIR_B200_OK) {
       q->nb_replies = reqs[i].nb_replies;
-      if (cudaMemcpyAsync(q->host_replies, dr[i], q->reply_bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+      if (cudaMemcpyAsync(q->host_replies, q->dr, q->reply_bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
         s = XPIR_B200_ERR_CUDA;
     }
     batch[i]->status = s;
   }
+  for (size_t i = 0; i < batch.size(); i++) {
+    auto *q = (ServedQuery *)batch[i]->payload.get();
+    if (q->dq) cudaFreeAsync(q->dq, st);
+    if (q->dr) cudaFreeAsync(q->dr, st);
+    q->dq = q->dr = nullptr;
+  }
   for (void *p : held) cudaFreeAsync(p, st);
   if (cudaStreamSynchronize(st) != cudaSuccess)
     for (auto *j : batch) j->status = XPIR_B200_ERR_CUDA;
+  if (q0->uploaded) cudaEventDestroy(q0->uploaded);
+  q0->uploaded = nullptr;
 }
 
 // Device bytes a query holds while admitted: its query and reply buffers and its share
@@ -158,8 +200,24 @@ int xpir_b200_server_create(xpir_b200_server **out, xpir_b200_ctx *const *ctxs, 
     }
     srv->pools.push_back(pool);
   }
-  srv->adm.reset(new xpir::Admission(nctx, device_budget_bytes, max_batch,
-                                     [srv](uint32_t lane, std::vector<xpir::Job *> &b) { run_batch(srv, lane, b); }));
+  for (uint32_t i = 0; i < nctx; i++) {
+    cudaStream_t cs = nullptr;
+    cudaError_t e = cudaSetDevice(ctxs[i]->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      for (cudaStream_t s2 : srv->copy_streams) cudaStreamDestroy(s2);
+      for (cudaMemPool_t p : srv->pools) cudaMemPoolDestroy(p);
+      delete srv;
+      return XPIR_B200_ERR_CUDA;
+    }
+    srv->copy_streams.push_back(cs);
+  }
+  // Two batches in flight per lane: one uploading while the previous one computes.
+  srv->adm.reset(new xpir::Admission(
+      nctx, device_budget_bytes, max_batch,
+      [srv](uint32_t lane, std::vector<xpir::Job *> &b) { upload_batch(srv, lane, b); },
+      [srv](uint32_t lane, std::vector<xpir::Job *> &b) { compute_batch(srv, lane, b); }, 2));
   *out = srv;
   return XPIR_B200_OK;
 }
@@ -221,6 +279,7 @@ int xpir_b200_server_stats(xpir_b200_server *srv, uint64_t *completed, uint64_t 
 int xpir_b200_server_destroy(xpir_b200_server *srv) {
   if (!srv) return XPIR_B200_ERR_ARG;
   srv->adm->stop();
+  for (cudaStream_t cs : srv->copy_streams) cudaStreamDestroy(cs);
   for (cudaMemPool_t p : srv->pools) cudaMemPoolDestroy(p);
   delete srv;
   return XPIR_B200_OK;
