@@ -194,6 +194,17 @@ XPIR_B200_API int xpir_b200_generate_query(xpir_b200_ctx *ctx, const uint8_t *pr
 XPIR_B200_API int xpir_b200_generate_secret_key(xpir_b200_ctx *ctx, const uint8_t *prng_key, uint64_t nonce,
                                                 uint64_t *secret_key);
 
+/* ---- optimizer costs ------------------------------------------------------------------- */
+/* The two per-plaintext costs XPIR's optimizer caches for a parameter set
+ * (PIROptimizer::getAbs1PlaintextTime / getPrecompute1PlaintextTime,
+ * pir/replyGenerator/PIROptimizer.cpp:155-209, with generateReplySimulation /
+ * precomputationSimulation, PIRReplyGeneratorNFL_internal.cpp:446-498), measured on this
+ * context's GPU: seconds of reply and of import per absorbed plaintext for a query over 4
+ * elements, the element size doubled until a reply takes target_s seconds (<= 0: 0.05 s)
+ * or the reference's 2^30-bit limit is reached. */
+XPIR_B200_API int xpir_b200_measure_costs(xpir_b200_ctx *ctx, uint32_t security_bits, double target_s,
+                                          double *reply_s_per_plaintext, double *import_s_per_plaintext);
+
 /* ---- serving loop ------------------------------------------------------------------ */
 /* A server over one or more contexts, one lane each.  Queries wait in FIFO order per
  * lane and are admitted while their device footprint (query, replies, recursion

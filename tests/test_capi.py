@@ -94,3 +94,11 @@ def test_admission_and_continuous_batching_host(tmp_path):
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert out.returncode == 0, out.stdout + out.stderr
     assert out.stdout.startswith("ok")
+
+
+def test_optimizer_cache_parameter_parsing():
+    from xpir_b200 import optim_cache
+
+    assert optim_cache.parse_params("LWE:80:2048:120") == (80, 2048, 2)
+    with pytest.raises(ValueError):
+        optim_cache.parse_params("LWE:80:2048:100")

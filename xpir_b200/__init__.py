@@ -93,6 +93,8 @@ def _load():
         L.xpir_b200_generate_query.argtypes = [vp, vp, c_u64, vp, c_u32, ctypes.POINTER(c_u32), c_u64, c_u32,
                                                 c_u32, vp, c_u64, ctypes.c_int]
         L.xpir_b200_generate_secret_key.argtypes = [vp, vp, c_u64, vp]
+        L.xpir_b200_measure_costs.argtypes = [vp, c_u32, ctypes.c_double, ctypes.POINTER(ctypes.c_double),
+                                              ctypes.POINTER(ctypes.c_double)]
         L.xpir_b200_server_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), c_u32, c_u64, c_u32]
         L.xpir_b200_server_submit.argtypes = [vp, vp, c_u32, ctypes.POINTER(c_u32), vp, vp, c_u64,
                                               ctypes.POINTER(c_u64)]
@@ -284,6 +286,14 @@ class Context:
         _check(_load().xpir_b200_extract(self.handle, sk.ctypes.data, d, b, aggregated_bytes, _ptr(replies), nrep,
                                          _on_device(replies), _ptr(out), cap, _on_device(out)), "extract")
         return out
+
+    def measure_costs(self, security_bits: int = 80, target_s: float = 0.05) -> tuple[float, float]:
+        """(reply, import) seconds per absorbed plaintext on this GPU, the two figures XPIR's
+        optimizer caches per parameter set."""
+        r, i = ctypes.c_double(), ctypes.c_double()
+        _check(_load().xpir_b200_measure_costs(self.handle, security_bits, target_s, ctypes.byref(r),
+                                               ctypes.byref(i)), "measure_costs")
+        return r.value, i.value
 
     def generate_secret_key(self, prng_key: np.ndarray, nonce: int = 0) -> np.ndarray:
         """NFLLWE key generation on the GPU from the PRNG call with `nonce`."""

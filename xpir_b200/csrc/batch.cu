@@ -399,3 +399,73 @@ extern "C" int xpir_b200_autotune(xpir_b200_ctx *ctx, const xpir_b200_db *db, ui
   if (e == cudaSuccess && *(volatile int *)ctx->status_host != 0) return XPIR_B200_ERR_TIMEOUT;
   return status_of(e);
 }
+
+// The optimizer's per-plaintext costs (pir/replyGenerator/PIROptimizer.cpp:155-209): a
+// one-dimensional query over n[0] = 4 elements of `plaintexts` polys each, doubled until
+// one reply takes `target_s` or the database reaches 2^30 ciphertext bits (the reference's
+// limit), then reply time and import time divided by the plaintexts in the database.
+extern "C" int xpir_b200_measure_costs(xpir_b200_ctx *ctx, uint32_t security_bits, double target_s,
+                                       double *reply_s_per_plaintext, double *import_s_per_plaintext) {
+  if (!ctx || !reply_s_per_plaintext || !import_s_per_plaintext || security_bits == 0) return XPIR_B200_ERR_ARG;
+  const uint32_t N = ctx->ps.N, m = ctx->ps.m, n0 = 4;
+  const int32_t b = xpir_b200_bits_per_coeff(N, m, security_bits, n0);
+  if (b <= 0) return XPIR_B200_ERR_ARG;
+  const uint64_t ct_bits = 2ull * 64 * m * N, abs_bytes = (uint64_t)b * N / 8;
+  if (target_s <= 0) target_s = 0.05;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return status_of(e);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  if (e != cudaSuccess) return status_of(e);
+  int rc = XPIR_B200_OK;
+  double reply_s = 0, import_s = 0;
+  uint64_t plaintexts = 4, used = 4;
+  std::vector<uint8_t> bytes;
+  std::vector<uint64_t> query((uint64_t)n0 * 2 * m * N, 1), replies;
+  for (;;) {
+    const uint64_t L = plaintexts * abs_bytes;
+    bytes.assign((uint64_t)n0 * L, 0x5a);
+    float ms_import = 0, ms_reply = 0;
+    xpir_b200_db *db = nullptr;
+    e = cudaEventRecord(e0, ctx->stream);
+    if (e == cudaSuccess) rc = xpir_b200_db_import(ctx, bytes.data(), n0, L, L, 1, (uint32_t)b, 0, &db);
+    if (e == cudaSuccess && rc == XPIR_B200_OK) e = cudaEventRecord(e1, ctx->stream);
+    if (e == cudaSuccess && rc == XPIR_B200_OK) e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess && rc == XPIR_B200_OK) e = cudaEventElapsedTime(&ms_import, e0, e1);
+    if (e == cudaSuccess && rc == XPIR_B200_OK) {
+      uint64_t P = 0, nagg = 0, dev = 0;
+      uint32_t bb = 0;
+      xpir_b200_db_info(db, &nagg, &P, &bb, &dev);
+      replies.assign(P * 2 * m * N, 0);
+      void *dq = nullptr, *dr = nullptr;
+      e = cudaMalloc(&dq, query.size() * 8);
+      if (e == cudaSuccess) e = cudaMalloc(&dr, replies.size() * 8);
+      if (e == cudaSuccess) e = cudaMemcpy(dq, query.data(), query.size() * 8, cudaMemcpyHostToDevice);
+      uint64_t cnt = 0;
+      for (int rep = 0; rep < 3 && e == cudaSuccess && rc == XPIR_B200_OK; rep++) {  // warm-up, then timed
+        if (rep == 2) e = cudaEventRecord(e0, ctx->stream);
+        rc = xpir_b200_reply(ctx, db, 1, &n0, dq, 1, dr, replies.size() * 8, 1, &cnt);
+        if (rep == 2 && e == cudaSuccess) e = cudaEventRecord(e1, ctx->stream);
+      }
+      if (e == cudaSuccess && rc == XPIR_B200_OK) e = cudaEventSynchronize(e1);
+      if (e == cudaSuccess && rc == XPIR_B200_OK) e = cudaEventElapsedTime(&ms_reply, e0, e1);
+      cudaFree(dq);
+      cudaFree(dr);
+    }
+    if (db) xpir_b200_db_free(db);
+    if (e != cudaSuccess || rc != XPIR_B200_OK) break;
+    reply_s = ms_reply / 1e3;
+    import_s = ms_import / 1e3;
+    used = plaintexts;
+    if (reply_s >= target_s || plaintexts * 2 * n0 * ct_bits >= (1ull << 30)) break;
+    plaintexts *= 2;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return status_of(e);
+  if (rc != XPIR_B200_OK) return rc;
+  *reply_s_per_plaintext = reply_s / ((double)n0 * used);
+  *import_s_per_plaintext = import_s / ((double)n0 * used);
+  return XPIR_B200_OK;
+}
