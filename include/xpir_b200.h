@@ -152,6 +152,15 @@ XPIR_B200_API int xpir_b200_reply_batch(xpir_b200_ctx *ctx, xpir_b200_request *r
 XPIR_B200_API int xpir_b200_autotune(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, const uint32_t *n,
                                      const void *query_dev, int *tile0);
 
+/* Pins the reply kernel's tile shape for one level shape (P polys per element, n_i slots
+ * per group, `groups` groups) on this context, as xpir_b200_autotune keeps its choice;
+ * tile -1 returns the shape to the default choice.  Tiles are numbered
+ * 0 .. xpir_b200_tile_count()-1; one that cannot run the shape is refused with
+ * XPIR_B200_ERR_ARG.  Replies do not depend on the tile.  No counterpart in the
+ * reference. */
+XPIR_B200_API int xpir_b200_set_level_tile(xpir_b200_ctx *ctx, uint64_t P, uint32_t n_i, uint64_t groups, int tile);
+XPIR_B200_API int xpir_b200_tile_count(void);
+
 /* ---- reply extraction (client side) ------------------------------------------------ */
 /* Ciphertexts decrypted at recursion level `level` (1 = innermost) for an aggregated
  * element of aggregated_bytes (alpha * element bytes): the float arithmetic of

@@ -16,10 +16,11 @@ def to_dev(torch, a):
 
 def mixed_batch(engine, ctx, torch):
     """Three databases of one parameter set queried with uneven shapes, as in the batched
-    configuration: d=1/alpha=1, d=1/alpha=4 (3 polys per element) and d=2."""
+    configuration: d=1/alpha=1, d=1/alpha=4 (3 polys per element), d=2, and d=2 with 9 of
+    24 level-0 groups idle in every query's row (their re-import is the constant fill)."""
     N, m, F, L = 2048, 2, 600, 3000  # alpha=4 gives 2 polys per element
     elems = random_db(77, F, L)
-    shapes = [([600], 1), ([150], 4), ([25, 24], 1)]
+    shapes = [([600], 1), ([150], 4), ([25, 24], 1), ([40, 24], 1)]
     dbs = []
     for n, alpha in shapes:
         b = engine.bits_per_coeff(N, m, n[0])

@@ -50,6 +50,8 @@ SHAPES = [
     (8192, 1, [6], 1, 6, 20000),          # largest degree
     (2048, 3, [64], 2, 100, 1500),        # alpha = 2, n0 not a multiple of the slot tile
     (512, 1, [1], 1, 1, 100),             # a single slot
+    (1024, 2, [4, 8, 3], 1, 9, 700),      # d = 3, 21 of 24 level-0 groups idle: constant re-import
+    (512, 3, [8, 5], 1, 3, 5000),         # P > 1, 4 of 5 level-0 groups idle
 ]
 
 
@@ -153,9 +155,8 @@ def test_launch_count_and_reuse(engine, oracle):
             q = random_query(100 + s, n, N, m, oracle.moduli(m))
             rep = ctx.reply(d, n, q)
             assert np.array_equal(rep, oracle.reply(imp, F, P, n, q, b, N, m))
-        # per reply: the level-0 query factors (4 groups share each slot), 2 level kernels
-        # and 1 re-import
-        assert ctx.launch_count - before == 3 * 4
+        # per reply: 2 level kernels and 1 re-import (every level-0 group holds data)
+        assert ctx.launch_count - before == 3 * 3
 
 
 def test_context_close_releases_databases(engine, oracle):

@@ -86,6 +86,8 @@ def _load():
                                       ctypes.c_int, ctypes.POINTER(c_u64)]
         L.xpir_b200_reply_batch.argtypes = [vp, ctypes.POINTER(Request), c_u32, ctypes.c_int]
         L.xpir_b200_autotune.argtypes = [vp, vp, c_u32, ctypes.POINTER(c_u32), vp, ctypes.POINTER(ctypes.c_int)]
+        L.xpir_b200_set_level_tile.argtypes = [vp, c_u64, c_u32, c_u64, ctypes.c_int]
+        L.xpir_b200_tile_count.argtypes = []
         L.xpir_b200_extract_count.restype = c_u64
         L.xpir_b200_extract_count.argtypes = [c_u64, c_u32, c_u32, c_u32, c_u32]
         L.xpir_b200_extract.argtypes = [vp, vp, c_u32, c_u32, c_u64, vp, c_u64, ctypes.c_int, vp, c_u64,
@@ -146,6 +148,11 @@ def ciphertext_bytes(N: int, m: int) -> int:
 def extract_count(aggregated_bytes: int, level: int, b: int, N: int, m: int) -> int:
     """Ciphertexts decrypted at recursion level `level` (the reply count at level d)."""
     return int(_load().xpir_b200_extract_count(aggregated_bytes, level, b, N, m))
+
+
+def tile_count() -> int:
+    """Number of compiled reply tile shapes (indices for Context.set_level_tile)."""
+    return _load().xpir_b200_tile_count()
 
 
 def modulus(i: int) -> int:
@@ -325,6 +332,10 @@ class Context:
         _check(_load().xpir_b200_autotune(self.handle, db.handle, len(n), narr, _ptr(query), ctypes.byref(tile)),
                "autotune")
         return tile.value
+
+    def set_level_tile(self, P: int, n_i: int, groups: int, tile: int) -> None:
+        """Pins the reply kernel's tile shape for one level shape (-1: default choice)."""
+        _check(_load().xpir_b200_set_level_tile(self.handle, P, n_i, groups, tile), "set_level_tile")
 
     def close(self) -> None:
         if self.handle:

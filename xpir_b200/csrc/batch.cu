@@ -71,14 +71,8 @@ struct Group {
 };
 
 struct Sizes {
-  size_t ws_a = 0, ws_b = 0, ws_f = 0, tasks = 0;
+  size_t ws_a = 0, ws_b = 0, tasks = 0;
 };
-
-// Whether level lvl of a group's queries reads precomputed query factors.
-bool group_level_factors(const Group &g, uint32_t lvl) {
-  const uint64_t real = lvl == 0 ? g.sh.n_real0 : g.sh.groups[lvl - 1];
-  return level_uses_factors(g.sh.P[lvl], active_groups(real, g.n[lvl], g.sh.groups[lvl]));
-}
 
 Sizes sizes_of(const xpir_b200_ctx *ctx, const std::vector<Group> &groups) {
   const uint64_t mN = (uint64_t)ctx->ps.m * ctx->ps.N, ct_bytes = 2 * mN * 8;
@@ -90,15 +84,13 @@ Sizes sizes_of(const xpir_b200_ctx *ctx, const std::vector<Group> &groups) {
       z.ws_a = std::max<size_t>(z.ws_a, k * g.sh.groups[lvl] * g.sh.P[lvl] * ct_bytes);
       z.ws_b = std::max<size_t>(z.ws_b, k * g.sh.groups[lvl] * g.sh.P[lvl + 1] * mN * 8);
     }
-    for (uint32_t lvl = 0; lvl < g.d; lvl++)
-      if (group_level_factors(g, lvl)) z.ws_f = std::max<size_t>(z.ws_f, k * (uint64_t)g.n[lvl] * ct_bytes);
   }
   return z;
 }
 
 // Enqueues every launch of the batch on the context's stream.
 cudaError_t enqueue(xpir_b200_ctx *ctx, const std::vector<Group> &groups, const xpir_b200_request *reqs,
-                    uint64_t *ws_a, uint64_t *ws_b, uint64_t *ws_f, ReplyTask *host_tasks, ReplyTask *dev_tasks) {
+                    uint64_t *ws_a, uint64_t *ws_b, ReplyTask *host_tasks, ReplyTask *dev_tasks) {
   const uint64_t mN = (uint64_t)ctx->ps.m * ctx->ps.N, ct_words = 2 * mN, ct_bytes = ct_words * 8;
   size_t task_off = 0;
   for (const Group &g : groups) {
@@ -106,7 +98,7 @@ cudaError_t enqueue(xpir_b200_ctx *ctx, const std::vector<Group> &groups, const 
     ps.b = g.db->b;
     const DevModuli dm = make_dev_moduli(ps);
     const uint32_t k = (uint32_t)g.reqs.size();
-    std::vector<const uint64_t *> db(k), q(k), f(k);
+    std::vector<const uint64_t *> db(k), q(k);
     std::vector<uint64_t *> out(k);
     uint64_t q_off = 0;
     for (uint32_t lvl = 0; lvl < g.d; lvl++) {
@@ -120,27 +112,22 @@ cudaError_t enqueue(xpir_b200_ctx *ctx, const std::vector<Group> &groups, const 
         out[i] = last ? (uint64_t *)r.replies : ws_a + (uint64_t)i * groups_l * P * ct_words;
       }
       uint32_t launched = 0;
-      cudaError_t e = cudaSuccess;
-      const bool use_f = group_level_factors(g, lvl);
-      for (uint32_t i = 0; i < k && use_f && e == cudaSuccess; i++) {
-        // Each query's level slots are shared by several groups: derive the factors once.
-        uint64_t *fi = ws_f + (uint64_t)i * g.n[lvl] * ct_words;
-        e = launch_query_factors(q[i], fi, g.n[lvl], ps, dm, ctx->stream, &launched);
-        f[i] = fi;
-      }
-      if (e == cudaSuccess)
-        e = launch_reply_tasks(db.data(), q.data(), use_f ? f.data() : nullptr, out.data(), k, n_real, P, groups_l,
-                               g.n[lvl], ps, dm, host_tasks + task_off, dev_tasks + task_off, ctx->stream, &launched,
-                               ctx->status_dev, tuned_tile(ctx, P, g.n[lvl], groups_l));
+      cudaError_t e = launch_reply_tasks(db.data(), q.data(), out.data(), k, n_real, P, groups_l, g.n[lvl], ps, dm,
+                                         host_tasks + task_off, dev_tasks + task_off, ctx->stream, &launched,
+                                         ctx->status_dev, tuned_tile(ctx, P, g.n[lvl], groups_l), last);
       ctx->launches += launched;
       if (e != cudaSuccess) return e;
       task_off += k;
       q_off += (uint64_t)g.n[lvl] * ct_words;
       if (last) break;
-      // All queries' level replies are one run of k*groups elements of P ciphertexts.
+      // All queries' level replies are one run of k*groups elements of P ciphertexts; in
+      // each query's row, groups past `active` replied exactly zero (and were not written).
       const AggSource as{(const uint8_t *)ws_a, (uint64_t)k * groups_l, P * ct_bytes, P * ct_bytes, 1};
-      e = launch_import(as, (uint64_t)k * groups_l, g.sh.P[lvl + 1], ps, dm, ctx->d_tables, ws_b, ctx->stream);
-      ctx->launches++;
+      const ImportRows rows{k, groups_l, active_groups(n_real, g.n[lvl], groups_l)};
+      launched = 0;
+      e = launch_import(as, (uint64_t)k * groups_l, g.sh.P[lvl + 1], ps, dm, ctx->d_tables, ws_b, ctx->stream,
+                        &rows, &launched);
+      ctx->launches += launched;
       if (e != cudaSuccess) return e;
     }
   }
@@ -154,7 +141,7 @@ cudaError_t enqueue(xpir_b200_ctx *ctx, const std::vector<Group> &groups, const 
 struct BatchPlan {
   std::vector<uint64_t> key;
   uint64_t launches = 0;  // engine kernels in the captured graph
-  void *ws_a = nullptr, *ws_b = nullptr, *ws_f = nullptr, *dev_tasks = nullptr, *host_tasks = nullptr;
+  void *ws_a = nullptr, *ws_b = nullptr, *dev_tasks = nullptr, *host_tasks = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   ~BatchPlan() {
@@ -162,7 +149,6 @@ struct BatchPlan {
     if (graph) cudaGraphDestroy(graph);
     cudaFree(ws_a);
     cudaFree(ws_b);
-    cudaFree(ws_f);
     cudaFree(dev_tasks);
     if (host_tasks) cudaFreeHost(host_tasks);
   }
@@ -246,9 +232,9 @@ int xpir::reply_batch_impl(xpir_b200_ctx *ctx, xpir_b200_request *reqs, uint32_t
     // Workspaces from the caller, or the context's own, grown on demand and kept; the
     // task table likewise.  After the first calls an uncaptured batch allocates and frees
     // nothing, so it never synchronises the device (other contexts' streams keep running).
-    void *wa = nullptr, *wb = nullptr, *wf = nullptr;
+    void *wa = nullptr, *wb = nullptr;
     if (workspace) {
-      if ((e = (*workspace)(z.ws_a, z.ws_b, z.ws_f, &wa, &wb, &wf)) != cudaSuccess) return finish(e);
+      if ((e = (*workspace)(z.ws_a, z.ws_b, &wa, &wb)) != cudaSuccess) return finish(e);
     } else {
       if (z.ws_a > ctx->ws_a_bytes) {
         cudaFree(ctx->ws_a);
@@ -264,16 +250,8 @@ int xpir::reply_batch_impl(xpir_b200_ctx *ctx, xpir_b200_request *reqs, uint32_t
         if ((e = cudaMalloc(&ctx->ws_b, z.ws_b)) != cudaSuccess) return finish(e);
         ctx->ws_b_bytes = z.ws_b;
       }
-      if (z.ws_f > ctx->ws_f_bytes) {
-        cudaFree(ctx->ws_f);
-        ctx->ws_f = nullptr;
-        ctx->ws_f_bytes = 0;
-        if ((e = cudaMalloc(&ctx->ws_f, z.ws_f)) != cudaSuccess) return finish(e);
-        ctx->ws_f_bytes = z.ws_f;
-      }
       wa = ctx->ws_a;
       wb = ctx->ws_b;
-      wf = ctx->ws_f;
     }
     if (z.tasks > ctx->tasks_cap) {
       cudaFree(ctx->tasks_dev);
@@ -288,7 +266,7 @@ int xpir::reply_batch_impl(xpir_b200_ctx *ctx, xpir_b200_request *reqs, uint32_t
     }
     // The pinned table may be rewritten here: the previous call on this context ended
     // with a stream synchronisation, so its copy has completed.
-    e = enqueue(ctx, groups, reqs, (uint64_t *)wa, (uint64_t *)wb, (uint64_t *)wf, (ReplyTask *)ctx->tasks_host,
+    e = enqueue(ctx, groups, reqs, (uint64_t *)wa, (uint64_t *)wb, (ReplyTask *)ctx->tasks_host,
                 (ReplyTask *)ctx->tasks_dev);
     return finish(e);
   }
@@ -304,20 +282,19 @@ int xpir::reply_batch_impl(xpir_b200_ctx *ctx, xpir_b200_request *reqs, uint32_t
   plan->key = key;
   e = cudaMalloc(&plan->ws_a, std::max<size_t>(z.ws_a, 256));
   if (e == cudaSuccess) e = cudaMalloc(&plan->ws_b, std::max<size_t>(z.ws_b, 256));
-  if (e == cudaSuccess) e = cudaMalloc(&plan->ws_f, std::max<size_t>(z.ws_f, 256));
   if (e == cudaSuccess) e = cudaMalloc(&plan->dev_tasks, z.tasks * sizeof(ReplyTask));
   if (e == cudaSuccess) e = cudaMallocHost(&plan->host_tasks, z.tasks * sizeof(ReplyTask));
   // One eager run first: it sets the kernels' attributes outside the capture and
   // produces this submission's replies.
   if (e == cudaSuccess)
-    e = enqueue(ctx, groups, reqs, (uint64_t *)plan->ws_a, (uint64_t *)plan->ws_b, (uint64_t *)plan->ws_f, (ReplyTask *)plan->host_tasks,
+    e = enqueue(ctx, groups, reqs, (uint64_t *)plan->ws_a, (uint64_t *)plan->ws_b, (ReplyTask *)plan->host_tasks,
                 (ReplyTask *)plan->dev_tasks);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e == cudaSuccess) e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     const uint64_t before = ctx->launches;
     const cudaError_t ee = enqueue(ctx, groups, reqs, (uint64_t *)plan->ws_a, (uint64_t *)plan->ws_b,
-                                   (uint64_t *)plan->ws_f, (ReplyTask *)plan->host_tasks, (ReplyTask *)plan->dev_tasks);
+                                   (ReplyTask *)plan->host_tasks, (ReplyTask *)plan->dev_tasks);
     plan->launches = ctx->launches - before;
     ctx->launches = before;  // captured, not launched
     e = cudaStreamEndCapture(ctx->stream, &plan->graph);
@@ -399,6 +376,21 @@ extern "C" int xpir_b200_autotune(xpir_b200_ctx *ctx, const xpir_b200_db *db, ui
   if (e == cudaSuccess && *(volatile int *)ctx->status_host != 0) return XPIR_B200_ERR_TIMEOUT;
   return status_of(e);
 }
+
+extern "C" int xpir_b200_set_level_tile(xpir_b200_ctx *ctx, uint64_t P, uint32_t n_i, uint64_t groups, int tile) {
+  if (!ctx || P == 0 || n_i == 0 || groups == 0) return XPIR_B200_ERR_ARG;
+  if (tile != -1 && !tile_fits(tile, P)) return XPIR_B200_ERR_ARG;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  const auto key = std::make_tuple(P, (uint64_t)n_i, groups);
+  if (tile == -1)
+    ctx->tuned.erase(key);
+  else
+    ctx->tuned[key] = tile;
+  ctx->tune_epoch++;
+  return XPIR_B200_OK;
+}
+
+extern "C" int xpir_b200_tile_count(void) { return tile_count(); }
 
 // The optimizer's per-plaintext costs (pir/replyGenerator/PIROptimizer.cpp:155-209): a
 // one-dimensional query over n[0] = 4 elements of `plaintexts` polys each, doubled until

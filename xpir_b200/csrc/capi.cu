@@ -162,7 +162,6 @@ int xpir_b200_ctx_destroy(xpir_b200_ctx *ctx) {
   cudaFree(ctx->ws_query);
   cudaFree(ctx->ws_a);
   cudaFree(ctx->ws_b);
-  cudaFree(ctx->ws_f);
   cudaFree(ctx->tasks_dev);
   if (ctx->tasks_host) cudaFreeHost(ctx->tasks_host);
   ctx->plans.clear();
@@ -301,15 +300,11 @@ int xpir_b200_reply(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, cons
 
   // Work out every level's shape first so that the workspaces grow at most once.
   uint64_t Ps[XPIR_B200_MAX_LEVELS], groups[XPIR_B200_MAX_LEVELS];
-  bool factors[XPIR_B200_MAX_LEVELS];
-  size_t need_a = 0, need_b = 0, need_f = 0;
+  size_t need_a = 0, need_b = 0;
   Ps[0] = db->P;
   for (uint32_t lvl = 0; lvl < d; lvl++) {
     groups[lvl] = 1;
     for (uint32_t j = lvl + 1; j < d; j++) groups[lvl] *= n[j];
-    const uint64_t real = lvl == 0 ? db->n_agg : groups[lvl - 1];
-    factors[lvl] = level_uses_factors(Ps[lvl], active_groups(real, n[lvl], groups[lvl]));
-    if (factors[lvl] && (uint64_t)n[lvl] * ct_bytes > need_f) need_f = (uint64_t)n[lvl] * ct_bytes;
     uint64_t rep_bytes;
     if (!mul_ok(groups[lvl] * Ps[lvl], ct_bytes, &rep_bytes)) return XPIR_B200_ERR_ARG;
     if (lvl + 1 < d) {
@@ -326,7 +321,6 @@ int xpir_b200_reply(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, cons
   int rc;
   if ((rc = grow(&ctx->ws_a, &ctx->ws_a_bytes, need_a)) != XPIR_B200_OK) return rc;
   if ((rc = grow(&ctx->ws_b, &ctx->ws_b_bytes, need_b)) != XPIR_B200_OK) return rc;
-  if ((rc = grow(&ctx->ws_f, &ctx->ws_f_bytes, need_f)) != XPIR_B200_OK) return rc;
 
   const uint64_t *dq = (const uint64_t *)query;
   if (!query_on_device) {
@@ -343,11 +337,8 @@ int xpir_b200_reply(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, cons
     uint64_t *rep = (last && out_on_device) ? (uint64_t *)replies : (uint64_t *)ctx->ws_a;
     uint32_t launched = 0;
     ReplyLevelArgs a{in, in_real, Ps[lvl], groups[lvl], n[lvl], dq, rep};
-    if (factors[lvl]) {
-      // The level's query is shared by several groups: derive its factors once.
-      XPIR_TRY(launch_query_factors(dq, (uint64_t *)ctx->ws_f, n[lvl], ps, dm, ctx->stream, &launched));
-      a.query_factors = (const uint64_t *)ctx->ws_f;
-    }
+    a.write_idle = last;
+    const uint64_t active = active_groups(in_real, n[lvl], groups[lvl]);
     const cudaError_t le = launch_reply_level(a, ps, dm, ctx->stream, &launched, ctx->status_dev,
                                               tuned_tile(ctx, Ps[lvl], n[lvl], groups[lvl]));
     if (le == cudaErrorNotSupported) return XPIR_B200_ERR_ARG;
@@ -357,10 +348,13 @@ int xpir_b200_reply(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, cons
     if (last) break;
     // Level replies -> next level's database: element e's Ps[lvl] ciphertexts are one
     // contiguous bit stream (no inverse NTT, as the reference).
+    // Groups past `active` replied exactly zero (and were not written out).
     const AggSource as{(const uint8_t *)rep, groups[lvl], Ps[lvl] * ct_bytes, Ps[lvl] * ct_bytes, 1};
+    const ImportRows rows{1, groups[lvl], active};
+    launched = 0;
     XPIR_TRY(launch_import(as, groups[lvl], Ps[lvl + 1], ps, dm, ctx->d_tables, (uint64_t *)ctx->ws_b,
-                           ctx->stream));
-    ctx->launches++;
+                           ctx->stream, &rows, &launched));
+    ctx->launches += launched;
     in = (const uint64_t *)ctx->ws_b;
     in_real = groups[lvl];
   }

@@ -34,8 +34,6 @@ struct xpir_b200_ctx {
   size_t ws_a_bytes = 0;
   void *ws_b = nullptr;  // re-imported level databases
   size_t ws_b_bytes = 0;
-  void *ws_f = nullptr;  // query Shoup factors of one level
-  size_t ws_f_bytes = 0;
   void *tasks_dev = nullptr;   // task table of uncaptured batches (device copy)
   void *tasks_host = nullptr;  // and its pinned staging copy
   size_t tasks_cap = 0;        // entries of both
@@ -68,9 +66,9 @@ struct xpir_b200_request;
 namespace xpir {
 
 // Supplies the workspace of an uncaptured batch: device buffers of at least `a` bytes
-// (level replies), `b` bytes (re-imported level databases) and `f` bytes (query factors),
-// valid in stream order on the context's stream until the batch call returns.
-typedef std::function<cudaError_t(size_t a, size_t b, size_t f, void **pa, void **pb, void **pf)> WorkspaceFn;
+// (level replies) and `b` bytes (re-imported level databases), valid in stream order on
+// the context's stream until the batch call returns.
+typedef std::function<cudaError_t(size_t a, size_t b, void **pa, void **pb)> WorkspaceFn;
 
 // xpir_b200_reply_batch with an optional workspace supplier (null: the context's own
 // cached workspaces).  Used by the serving loop to draw workspaces from its budgeted pool.

@@ -8,6 +8,7 @@
 //
 // HBM layout of the output: [element][poly][modulus][coefficient] u64, values in [0, 2p).
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <stdint.h>
 
 #include "kernels.h"
@@ -32,11 +33,16 @@ DevModuli make_dev_moduli(const ParamSet &ps) {
 
 namespace {
 
-constexpr int kImportThreads = 256;
+// Threads per import CTA: N/16, two 8-coefficient groups of the register-blocked NTT
+// per thread and pass (on B200 this beat one group per thread, 16-coefficient groups,
+// and the transform fed straight from the bit extraction, all bit-identical).
+constexpr uint32_t kImportMaxThreads = kMaxPolyDegree / 16;
+inline uint32_t import_threads(uint32_t N) { return N / 16; }
 
 struct ImportShape {
   uint32_t N, log_n, m, b, nsub;
   uint64_t P;
+  uint64_t per_row, active;  // element s of CTA u = blockIdx.x / P: (u / active) * per_row + u % active
   uint64_t total_bytes;  // bytes of one aggregated element (alpha * element_bytes)
   uint32_t stage_words;  // u64 words of staged input per poly
 };
@@ -72,15 +78,17 @@ __device__ __forceinline__ uint64_t staged_bits(const uint64_t *st, uint64_t pos
   return v & ((1ull << nbits) - 1);
 }
 
-// grid: x = aggregated element * P + poly, y = modulus.  Dynamic smem: stage words, then N words.
-__global__ void __launch_bounds__(kImportThreads) import_kernel(const AggSource src, const ImportShape sh,
-                                                                const DevModuli dm,
-                                                                const uint64_t *__restrict__ tables,
-                                                                uint64_t *__restrict__ out) {
+// grid: x = aggregated element * P + poly, y = modulus; import_threads(N) threads.
+// Dynamic smem: stage words, then N words.
+__global__ void __launch_bounds__(kImportMaxThreads) import_kernel(const AggSource src, const ImportShape sh,
+                                                                   const DevModuli dm,
+                                                                   const uint64_t *__restrict__ tables,
+                                                                   uint64_t *__restrict__ out) {
   extern __shared__ __align__(16) uint64_t smem[];
   uint64_t *stage = smem;
   uint64_t *poly = smem + sh.stage_words;
-  const uint64_t s = blockIdx.x / sh.P, j = blockIdx.x - s * sh.P;
+  const uint64_t u = blockIdx.x / sh.P, j = blockIdx.x - u * sh.P;
+  const uint64_t row = u / sh.active, s = row * sh.per_row + (u - row * sh.active);
   const uint32_t c = blockIdx.y;
   const uint32_t N = sh.N;
   const uint64_t p = dm.p[c];
@@ -111,8 +119,9 @@ __global__ void __launch_bounds__(kImportThreads) import_kernel(const AggSource 
   }
   __syncthreads();
 
-  // Coefficients: b <= 56 one chunk per coefficient; b > 56 sub-chunks of 56 bits
-  // combined per modulus as sum_t mulmod(s_t, 2^(56t)) without a final reduction.
+  // Coefficient k, twisted by phi^k: b <= 56 one chunk per coefficient; b > 56 sub-chunks
+  // of 56 bits combined per modulus as sum_t mulmod(s_t, 2^(56t)) without a final
+  // reduction.
   const uint64_t *tab = tables + (uint64_t)c * kTableSlots * N;
   const uint64_t *phi = tab + kPhi * N, *phi_s = tab + kPhiShoup * N;
   const uint64_t rel0 = bit0 - 8 * byte0;
@@ -129,19 +138,58 @@ __global__ void __launch_bounds__(kImportThreads) import_kernel(const AggSource 
         x += shoup_mul(sub, dm.crt[c][t], dm.crt_shoup[c][t], p);
       }
     }
-    poly[k] = shoup_mul(x, __ldg(phi + k), __ldg(phi_s + k), p);
+    poly[swz(k)] = shoup_mul(x, __ldg(phi + k), __ldg(phi_s + k), p);
   }
-  ntt_lazy_smem(poly, tab + kOmega * N, tab + kOmegaShoup * N, N, sh.log_n, p);
+  __syncthreads();
+  ntt_lazy_rb<3>(poly, tab + kOmega * N, tab + kOmegaShoup * N, N, sh.log_n, p,
+                 [&](uint32_t k) { return poly[swz(k)]; });
 
-  uint64_t *o = out + ((s * sh.P + j) * sh.m + c) * (uint64_t)N;
-  for (uint32_t k = threadIdx.x; k < N; k += blockDim.x) o[k] = poly[k];
+  // Coalesced 16-byte stores; swz(2t+1) == swz(2t) ^ 1.
+  ulonglong2 *o = reinterpret_cast<ulonglong2 *>(out + ((s * sh.P + j) * sh.m + c) * (uint64_t)N);
+  for (uint32_t t = threadIdx.x; t < N / 2; t += blockDim.x) {
+    const uint32_t at = swz(2 * t);
+    o[t] = make_ulonglong2(poly[at], poly[at ^ 1]);
+  }
+}
+
+// The import of an all-zero bit stream, broadcast: every coefficient chunk is 0, so the
+// twisted coefficients are 0 and the lazy NTT leaves one fixed poly per modulus (values
+// 0 and p).  Each CTA computes it for modulus blockIdx.y in shared memory, then writes it
+// to its share of the `count` known-zero polys t (element row * per_row + active +
+// (t / P) % (per_row - active) of row t / (P * (per_row - active)), poly t % P).
+__global__ void __launch_bounds__(kImportMaxThreads) import_zero_fill_kernel(const ImportShape sh,
+                                                                             const DevModuli dm,
+                                                                             const uint64_t *__restrict__ tables,
+                                                                             uint64_t *__restrict__ out,
+                                                                             uint64_t count) {
+  extern __shared__ __align__(16) uint64_t smem[];
+  const uint32_t c = blockIdx.y, N = sh.N;
+  const uint64_t p = dm.p[c];
+  const uint64_t *tab = tables + (uint64_t)c * kTableSlots * N;
+  const uint64_t *phi = tab + kPhi * N, *phi_s = tab + kPhiShoup * N;
+  auto coefficient = [&](uint32_t k) -> uint64_t { return shoup_mul(0, __ldg(phi + k), __ldg(phi_s + k), p); };
+  ntt_lazy_rb<3>(smem, tab + kOmega * N, tab + kOmegaShoup * N, N, sh.log_n, p, coefficient);
+  const uint64_t zeros = sh.per_row - sh.active;
+  for (uint64_t t = blockIdx.x; t < count; t += gridDim.x) {
+    const uint64_t u = t / sh.P, j = t - u * sh.P;
+    const uint64_t row = u / zeros, s = row * sh.per_row + sh.active + (u - row * zeros);
+    ulonglong2 *o = reinterpret_cast<ulonglong2 *>(out + ((s * sh.P + j) * sh.m + c) * (uint64_t)N);
+    for (uint32_t i = threadIdx.x; i < N / 2; i += blockDim.x) {
+      const uint32_t at = swz(2 * i);
+      o[i] = make_ulonglong2(smem[at], smem[at ^ 1]);
+    }
+  }
 }
 
 }  // namespace
 
 cudaError_t launch_import(const AggSource &src, uint64_t groups, uint64_t P, const ParamSet &ps,
-                          const DevModuli &dm, const uint64_t *tables, uint64_t *out, cudaStream_t stream) {
+                          const DevModuli &dm, const uint64_t *tables, uint64_t *out, cudaStream_t stream,
+                          const ImportRows *rows, uint32_t *launches) {
   if (groups == 0 || P == 0) return cudaSuccess;
+  const ImportRows r = rows ? *rows : ImportRows{1, groups, groups};
+  if (r.rows == 0 || r.per_row == 0 || r.rows * r.per_row != groups || r.active > r.per_row)
+    return cudaErrorInvalidValue;
   ImportShape sh;
   sh.N = ps.N;
   sh.log_n = ps.log_n;
@@ -149,17 +197,40 @@ cudaError_t launch_import(const AggSource &src, uint64_t groups, uint64_t P, con
   sh.b = ps.b;
   sh.nsub = (ps.b + 55) / 56;
   sh.P = P;
+  sh.per_row = r.per_row;
+  sh.active = r.active;
   sh.total_bytes = (uint64_t)src.alpha * src.element_bytes;
   // bits of one poly plus the in-word offset, rounded up, plus one spare word for the
   // two-word reads of staged_bits
   sh.stage_words = (uint32_t)((64 + (uint64_t)ps.N * ps.b + 63) / 64 + 2);
   const size_t smem = (size_t)(sh.stage_words + ps.N) * sizeof(uint64_t);
-  cudaError_t e = cudaFuncSetAttribute(import_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  if (groups * P > 0x7fffffffull) return cudaErrorInvalidValue;
-  dim3 grid((unsigned)(groups * P), ps.m);
-  import_kernel<<<grid, kImportThreads, smem, stream>>>(src, sh, dm, tables, out);
-  return cudaGetLastError();
+  const unsigned threads = import_threads(ps.N);
+  const uint64_t computed = r.rows * r.active, zero_polys = r.rows * (r.per_row - r.active) * P;
+  if (computed * P > 0x7fffffffull) return cudaErrorInvalidValue;
+  if (computed > 0) {
+    cudaError_t e = cudaFuncSetAttribute(import_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid((unsigned)(computed * P), ps.m);
+    import_kernel<<<grid, threads, smem, stream>>>(src, sh, dm, tables, out);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (launches) (*launches)++;
+  }
+  if (zero_polys > 0) {
+    const size_t zsmem = (size_t)ps.N * sizeof(uint64_t);
+    cudaError_t e = cudaFuncSetAttribute(import_zero_fill_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)zsmem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    // About four CTAs per SM over all moduli: each computes the constant poly once.
+    const uint64_t per_mod = std::max<uint64_t>(1, 4ull * (uint64_t)sms / ps.m);
+    dim3 grid((unsigned)std::min<uint64_t>(zero_polys, per_mod), ps.m);
+    import_zero_fill_kernel<<<grid, threads, zsmem, stream>>>(sh, dm, tables, out, zero_polys);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (launches) (*launches)++;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace xpir

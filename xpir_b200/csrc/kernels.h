@@ -39,8 +39,20 @@ DevModuli make_dev_moduli(const ParamSet &ps);
 // phi-twist + forward NTT into out[(s*P + j)][m][N].  groups = ceil(nb/alpha),
 // P = polys_for_bits(8*alpha*element_bytes, b, N).  `tables` is the device copy of the
 // ParamSet tables.  Returns a CUDA error code.
+//
+// With `rows`, the groups elements form rows->rows rows of rows->per_row, and in each row
+// only the first rows->active elements carry data: the rest are known all-zero bit
+// streams (level replies of groups that had no real slot, which are exactly zero).  All
+// their polys import to one constant poly per modulus -- not zero: the lazy butterflies
+// turn zeros into multiples of p -- which a fill kernel computes once per CTA and
+// broadcasts instead of running the import on each.  *launches (if given) is increased
+// by the kernels launched.
+struct ImportRows {
+  uint64_t rows, per_row, active;
+};
 cudaError_t launch_import(const AggSource &src, uint64_t groups, uint64_t P, const ParamSet &ps,
-                          const DevModuli &dm, const uint64_t *tables, uint64_t *out, cudaStream_t stream);
+                          const DevModuli &dm, const uint64_t *tables, uint64_t *out, cudaStream_t stream,
+                          const ImportRows *rows = nullptr, uint32_t *launches = nullptr);
 
 // One recursion level of the reply (pir/replyGenerator/PIRReplyGeneratorNFL_internal.cpp:511-595):
 // for group g < n_groups and poly cp < P, the in-order lazy Shoup accumulation over the
@@ -54,9 +66,10 @@ struct ReplyLevelArgs {
   uint64_t n_i;
   const uint64_t *query;  // [n_i][2][m][N]
   uint64_t *out;
-  // The query's Shoup factors (same layout), from launch_query_factors, or null to derive
-  // them in the kernel.  Used by one-poly levels (P = 1).
-  const uint64_t *query_factors = nullptr;
+  // Whether the replies of groups without a real slot (exactly zero) are written out.
+  // A level whose replies only feed the next level's import (which knows they are zero,
+  // see ImportRows) skips it.
+  bool write_idle = true;
 };
 // `status` is a device-visible int that a kernel sets to a nonzero KernelStatus when one
 // of its bounded waits gives up (sm100.cuh); the caller clears and reads it.
@@ -70,48 +83,41 @@ cudaError_t launch_reply_level(const ReplyLevelArgs &a, const ParamSet &ps, cons
 struct alignas(128) ReplyTask {
   CUtensorMap tm_db;
   CUtensorMap tm_q;
-  CUtensorMap tm_qf;  // query factors (tiles that read them)
   uint64_t *out;
 };
 
-// A compiled tile shape of the reply kernel: W coefficients per slice, C poly columns
-// per CTA, E slots per tile, NS pipeline stages, TB term buffers, IPT slot pairs per
-// compute thread, pre: reads precomputed query factors.
+// A compiled tile shape of the reply kernel: W coefficients per slice, C columns per
+// CTA, E slots per tile, NS pipeline stages, TB term buffers, IPT slot pairs per
+// compute thread; the columns are polys of one element, or with grp groups of a
+// one-poly level.
 struct TileShape {
   int W, C, E, NS, TB, IPT;
-  bool pre;
+  bool grp;
 };
-// Index of the default shape for a level with P polys per element, degree N, m moduli
-// and `ctas_per_slice` CTAs per (coefficient slice, modulus) (active groups x tasks).
-int default_tile(uint64_t P, uint32_t N, uint32_t m, uint64_t ctas_per_slice);
+// Index of the default shape for a level with P polys per element, degree N, m moduli,
+// `groups` active groups per task and `ntasks` tasks in the launch.
+int default_tile(uint64_t P, uint32_t N, uint32_t m, uint64_t groups, uint64_t ntasks);
 // Shapes the autotuner may try for a level with P polys per element.
 std::vector<int> tile_candidates(uint64_t P);
 TileShape tile_shape(int tile);
 int tile_count();
+// Whether a tile can run a level with P polys per element.
+bool tile_fits(int tile, uint64_t P);
 
 // `ntasks` reply levels of the same shape (n_real, P, n_groups, n_i), one per query,
 // in one launch.  `host_tasks` (pinned, ntasks entries) is filled here and copied to
 // `dev_tasks` on `stream` before the launch.  tile < 0 picks the default shape.
-cudaError_t launch_reply_tasks(const uint64_t *const *db, const uint64_t *const *query,
-                               const uint64_t *const *factors, uint64_t *const *out, uint32_t ntasks, uint64_t n_real,
+cudaError_t launch_reply_tasks(const uint64_t *const *db, const uint64_t *const *query, uint64_t *const *out,
+                               uint32_t ntasks, uint64_t n_real,
                                uint64_t P, uint64_t n_groups, uint64_t n_i, const ParamSet &ps, const DevModuli &dm,
                                ReplyTask *host_tasks, ReplyTask *dev_tasks, cudaStream_t stream, uint32_t *launches,
-                               int *status, int tile);
+                               int *status, int tile, bool write_idle = true);
 
 // Groups of a level that hold at least one real element (the others reply exactly zero).
 inline uint64_t active_groups(uint64_t n_real, uint64_t n_i, uint64_t n_groups) {
   const uint64_t a = n_i == 0 ? 0 : (n_real + n_i - 1) / n_i;
   return a < n_groups ? a : n_groups;
 }
-
-// Whether a level should read precomputed query factors: one poly per element and at
-// least four groups sharing each query slot, so that deriving every factor once (one
-// memory-bound pass) replaces deriving it once per group inside the reply kernel.
-inline bool level_uses_factors(uint64_t P, uint64_t active) { return P == 1 && active >= 4; }
-
-// The Shoup factors of n_ct query ciphertexts into `factors` (same layout and size).
-cudaError_t launch_query_factors(const uint64_t *query, uint64_t *factors, uint64_t n_ct, const ParamSet &ps,
-                                 const DevModuli &dm, cudaStream_t stream, uint32_t *launches);
 
 // Whether the reply kernel supports this level shape (moduli with the fast Shoup-factor
 // path, degree a multiple of 16, 32-bit TMA coordinates).

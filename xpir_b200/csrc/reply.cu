@@ -40,25 +40,26 @@
 namespace xpir {
 namespace {
 
-// Tile configuration: W coefficients per slice, C poly columns, E slots per tile, NS
-// pipeline stages, TB term buffers, IPT slot pairs per compute thread and tile, PRE:
-// the query's Shoup factors come precomputed from memory (a third TMA box per stage)
-// instead of being derived in the tile.  One chain thread per (half, column, coefficient).
-template <int W, int C, int E, int NS, int TB = 2, int IPT = 1, bool PRE = false>
+// Tile configuration: W coefficients per slice, C columns, E slots per tile, NS
+// pipeline stages, TB term buffers, IPT slot pairs per compute thread and tile.  The C
+// columns are C consecutive polys of one element, or with GRP (one-poly levels) the same
+// poly of C consecutive groups, which then share every query tile and the Shoup factors
+// derived from it.  One chain thread per (half, column, coefficient).
+template <int W, int C, int E, int NS, int TB = 2, int IPT = 1, bool GRP = false>
 struct Cfg {
   static constexpr int kComputeWarps = E * W / 2 / 32 / IPT;
   static constexpr int kComputeThreads = 32 * kComputeWarps;
   static constexpr int kChainThreads = 2 * C * W;
   static constexpr int kChainWarps = (kChainThreads + 31) / 32;
   static constexpr int kThreads = 32 * (1 + kComputeWarps + kChainWarps);
-  static constexpr int kX = E * C * W;     // DB box    [E][C][W]
-  static constexpr int kQ = E * 2 * W;     // query box [E][2][W] (and factor box)
-  static constexpr int kQF = PRE ? kQ : 0;
+  static constexpr int kX = E * C * W;     // DB box    [E][C][W], with GRP [C][E][W]
+  static constexpr int kQ = E * 2 * W;     // query box [E][2][W]
   static constexpr int kT = 2 * C * E * W;  // terms     [half][C][E/2][W][2] per buffer
-  static constexpr size_t kBytes = (size_t)(NS * (kX + kQ + kQF) + TB * kT) * 8 + (2 * NS + 2 * TB) * 8;
+  static constexpr size_t kBytes = (size_t)(NS * (kX + kQ) + TB * kT) * 8 + (2 * NS + 2 * TB) * 8;
   static_assert((TB & (TB - 1)) == 0, "term buffers: a power of two");
   static_assert(E % 2 == 0 && (E * W / 2) % (32 * IPT) == 0, "slot pairs must fill whole warps");
   static_assert((W * 8) % 16 == 0, "TMA rows must be multiples of 16 bytes");
+  static_assert(!GRP || C > 1, "group columns: at least two groups");
 };
 
 // 16-byte shared-memory load/store of two consecutive words.  volatile keeps a batch of
@@ -78,6 +79,7 @@ __device__ __forceinline__ void st_v2(uint64_t *p, uint64_t a, uint64_t b) {
 struct LevelShape {
   uint64_t n_real, P, n_i;
   uint32_t N, m, col_blocks;
+  uint64_t groups;  // groups with data (GRP tiles write only these)
 };
 
 
@@ -85,19 +87,18 @@ struct LevelShape {
 // blockIdx.z, with the DB and query tensor maps and the output of its task.  The last
 // slice may extend past N (W need not divide N): the TMA fills those coefficients with
 // zeros and their chains write nothing.
-template <int W, int C, int E, int NS, int TB, int IPT, bool PRE>
+template <int W, int C, int E, int NS, int TB, int IPT, bool GRP>
 __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUtensorMap *tm_q,
-                                           const CUtensorMap *tm_qf, uint64_t *__restrict__ out, const uint64_t g,
+                                           uint64_t *__restrict__ out, const uint64_t g,
                                            const LevelShape &sh, const DevModuli &dm, int *status) {
-  using S = Cfg<W, C, E, NS, TB, IPT, PRE>;
+  using S = Cfg<W, C, E, NS, TB, IPT, GRP>;
   constexpr int kComputeWarps = S::kComputeWarps;
   constexpr int kComputeThreads = S::kComputeThreads;
   constexpr int kW = W;
   extern __shared__ __align__(128) uint64_t sm[];
   uint64_t *xs = sm;                         // [NS][E][C][W]
   uint64_t *qs = xs + NS * S::kX;            // [NS][E][2][W]
-  uint64_t *qfs = qs + NS * S::kQ;           // [NS][E][2][W] when PRE
-  uint64_t *terms = qfs + NS * S::kQF;       // [TB][2][C][E/2][W][2]
+  uint64_t *terms = qs + NS * S::kQ;         // [TB][2][C][E/2][W][2]
   uint64_t *bars = terms + TB * S::kT;
   uint64_t *full = bars, *empty = bars + NS, *tfull = bars + 2 * NS, *tempty = bars + 2 * NS + TB;
 
@@ -131,8 +132,7 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
     if (lane == 0) {
       tma_prefetch_desc(tm_db);
       tma_prefetch_desc(tm_q);
-      if constexpr (PRE) tma_prefetch_desc(tm_qf);
-      constexpr uint32_t kTx = (uint32_t)((S::kX + S::kQ + S::kQF) * 8);
+      constexpr uint32_t kTx = (uint32_t)((S::kX + S::kQ) * 8);
       uint32_t t = 0;
       for (; t < tiles; ++t) {
         const int s = (int)(t % NS);
@@ -142,9 +142,15 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
         }
         mbar_arrive_expect_tx(full + s, kTx);
         const int slot = (int)t * E;
-        tma_load_4d(xs + s * S::kX, tm_db, k0, (int)c, (int)cp0, (int)(g * sh.n_i) + slot, full + s);
+        if constexpr (GRP) {
+#pragma unroll
+          for (int col = 0; col < C; col++)
+            tma_load_4d(xs + s * S::kX + col * E * kW, tm_db, k0, (int)c, 0, (int)((g * C + col) * sh.n_i) + slot,
+                        full + s);
+        } else {
+          tma_load_4d(xs + s * S::kX, tm_db, k0, (int)c, (int)cp0, (int)(g * sh.n_i) + slot, full + s);
+        }
         tma_load_4d(qs + s * S::kQ, tm_q, k0, (int)c, 0, slot, full + s);
-        if constexpr (PRE) tma_load_4d(qfs + s * S::kQF, tm_qf, k0, (int)c, 0, slot, full + s);
       }
       // Drain: every issued copy must have landed before the CTA exits.
       const uint32_t first = t > (uint32_t)NS ? t - NS : 0;
@@ -160,7 +166,6 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
       if (!ok) break;
       const uint64_t *xst = xs + s * S::kX;
       const uint64_t *qst = qs + s * S::kQ;
-      const uint64_t *qfst = qfs + s * S::kQF;
       uint64_t *tb = terms + b * S::kT;
       // Thread -> IPT items (coefficient k, slot pair e, e+1); the pair is stored as one
       // 16-byte word so that a chain thread reads two consecutive slots with one load.
@@ -177,17 +182,16 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
           const uint64_t ya1 = qst[(e * 2 + 2) * kW + k], yb1 = qst[(e * 2 + 3) * kW + k];
 #pragma unroll
           for (int col = 0; col < C; col++) {
-            x[col][0] = xst[(e * C + col) * kW + k];
-            x[col][1] = xst[((e + 1) * C + col) * kW + k];
+            if constexpr (GRP) {
+              x[col][0] = xst[(col * E + e) * kW + k];
+              x[col][1] = xst[(col * E + e + 1) * kW + k];
+            } else {
+              x[col][0] = xst[(e * C + col) * kW + k];
+              x[col][1] = xst[((e + 1) * C + col) * kW + k];
+            }
           }
-          uint64_t ysa0, ysb0, ysa1, ysb1;
-          if constexpr (PRE) {
-            ysa0 = qfst[(e * 2 + 0) * kW + k], ysb0 = qfst[(e * 2 + 1) * kW + k];
-            ysa1 = qfst[(e * 2 + 2) * kW + k], ysb1 = qfst[(e * 2 + 3) * kW + k];
-          } else {
-            ysa0 = shoup_factor8_np(ya0, p, np, delta), ysb0 = shoup_factor8_np(yb0, p, np, delta);
-            ysa1 = shoup_factor8_np(ya1, p, np, delta), ysb1 = shoup_factor8_np(yb1, p, np, delta);
-          }
+          const uint64_t ysa0 = shoup_factor8_np(ya0, p, np, delta), ysb0 = shoup_factor8_np(yb0, p, np, delta);
+          const uint64_t ysa1 = shoup_factor8_np(ya1, p, np, delta), ysb1 = shoup_factor8_np(yb1, p, np, delta);
 #pragma unroll
           for (int col = 0; col < C; col++) {
             const uint64_t x0 = x[col][0], x1 = x[col][1];
@@ -204,14 +208,8 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
           const int k = item % kW, ep = item / kW, e = 2 * ep;
           const uint64_t ya0 = qst[(e * 2 + 0) * kW + k], yb0 = qst[(e * 2 + 1) * kW + k];
           const uint64_t ya1 = qst[(e * 2 + 2) * kW + k], yb1 = qst[(e * 2 + 3) * kW + k];
-          uint64_t ysa0, ysb0, ysa1, ysb1;
-          if constexpr (PRE) {
-            ysa0 = qfst[(e * 2 + 0) * kW + k], ysb0 = qfst[(e * 2 + 1) * kW + k];
-            ysa1 = qfst[(e * 2 + 2) * kW + k], ysb1 = qfst[(e * 2 + 3) * kW + k];
-          } else {
-            ysa0 = shoup_factor8_np(ya0, p, np, delta), ysb0 = shoup_factor8_np(yb0, p, np, delta);
-            ysa1 = shoup_factor8_np(ya1, p, np, delta), ysb1 = shoup_factor8_np(yb1, p, np, delta);
-          }
+          const uint64_t ysa0 = shoup_factor8_np(ya0, p, np, delta), ysb0 = shoup_factor8_np(yb0, p, np, delta);
+          const uint64_t ysa1 = shoup_factor8_np(ya1, p, np, delta), ysb1 = shoup_factor8_np(yb1, p, np, delta);
           const uint64_t x0 = xst[e * kW + k], x1 = xst[(e + 1) * kW + k];
           sts_v2(tb + (ep * kW + k) * 2, shoup_lazy_np(x0, ya0, ysa0, np), shoup_lazy_np(x1, ya1, ysa1, np));
           sts_v2(tb + (((E / 2) + ep) * kW + k) * 2, shoup_lazy_np(x0, yb0, ysb0, np), shoup_lazy_np(x1, yb1, ysb1, np));
@@ -264,10 +262,13 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
       }
       mbar_arrive(tempty + b);
     }
-    const uint64_t cp = cp0 + col;
-    if (ok && cp < sh.P && k0 + k < (int)sh.N) {
-      const uint64_t mN = (uint64_t)sh.m * sh.N;
-      out[((g * sh.P + cp) * 2 + h) * mN + (uint64_t)c * sh.N + k0 + k] = rop;
+    const uint64_t mN = (uint64_t)sh.m * sh.N;
+    if constexpr (GRP) {
+      const uint64_t grp = g * C + col;  // one poly per element
+      if (ok && grp < sh.groups && k0 + k < (int)sh.N) out[(grp * 2 + h) * mN + (uint64_t)c * sh.N + k0 + k] = rop;
+    } else {
+      const uint64_t cp = cp0 + col;
+      if (ok && cp < sh.P && k0 + k < (int)sh.N) out[((g * sh.P + cp) * 2 + h) * mN + (uint64_t)c * sh.N + k0 + k] = rop;
     }
   }
   if (!ok) {
@@ -277,118 +278,98 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
 }
 
 // Two CTAs per SM for the narrow tiles (shared memory allows it), one for the wide ones.
-template <int W, int C, int E, int NS, int TB, int IPT, bool PRE>
+template <int W, int C, int E, int NS, int TB, int IPT, bool GRP>
 constexpr int min_blocks() {
-  return (C <= 2 && Cfg<W, C, E, NS, TB, IPT, PRE>::kThreads <= 640) ? 2 : 1;
+  return ((C <= 2 || (GRP && C <= 4)) && Cfg<W, C, E, NS, TB, IPT, GRP>::kThreads <= 640) ? 2 : 1;
 }
 
-// One query: tensor maps as grid constants (tm_qf only read when PRE).  Grid: x = group.
-template <int W, int C, int E, int NS, int TB, int IPT, bool PRE>
-__global__ void __launch_bounds__(Cfg<W, C, E, NS, TB, IPT, PRE>::kThreads, min_blocks<W, C, E, NS, TB, IPT, PRE>())
+// One query: tensor maps as grid constants.  Grid: x = group (GRP: block of C groups).
+template <int W, int C, int E, int NS, int TB, int IPT, bool GRP>
+__global__ void __launch_bounds__(Cfg<W, C, E, NS, TB, IPT, GRP>::kThreads, min_blocks<W, C, E, NS, TB, IPT, GRP>())
     reply_tma_kernel(const __grid_constant__ CUtensorMap tm_db, const __grid_constant__ CUtensorMap tm_q,
-                     const __grid_constant__ CUtensorMap tm_qf, uint64_t *__restrict__ out, const LevelShape sh,
+                     uint64_t *__restrict__ out, const LevelShape sh,
                      const DevModuli dm, int *status) {
-  reply_tile<W, C, E, NS, TB, IPT, PRE>(&tm_db, &tm_q, &tm_qf, out, blockIdx.x, sh, dm, status);
+  reply_tile<W, C, E, NS, TB, IPT, GRP>(&tm_db, &tm_q, out, blockIdx.x, sh, dm, status);
 }
 
 // Several tasks of one level shape (a batch of queries): each task's tensor maps and
 // output come from a descriptor table in global memory.  Grid: x = group * tasks + task,
 // so the CTAs of all queries that read the same DB tile run side by side and share it
 // through L2.
-template <int W, int C, int E, int NS, int TB, int IPT, bool PRE>
-__global__ void __launch_bounds__(Cfg<W, C, E, NS, TB, IPT, PRE>::kThreads, min_blocks<W, C, E, NS, TB, IPT, PRE>())
+template <int W, int C, int E, int NS, int TB, int IPT, bool GRP>
+__global__ void __launch_bounds__(Cfg<W, C, E, NS, TB, IPT, GRP>::kThreads, min_blocks<W, C, E, NS, TB, IPT, GRP>())
     reply_tma_tasks_kernel(const ReplyTask *__restrict__ tasks, const uint32_t ntasks, const LevelShape sh,
                            const DevModuli dm, int *status) {
   const uint32_t t = blockIdx.x % ntasks;
-  reply_tile<W, C, E, NS, TB, IPT, PRE>(&tasks[t].tm_db, &tasks[t].tm_q, &tasks[t].tm_qf, tasks[t].out,
+  reply_tile<W, C, E, NS, TB, IPT, GRP>(&tasks[t].tm_db, &tasks[t].tm_q, tasks[t].out,
                                         blockIdx.x / ntasks, sh, dm, status);
 }
 
-// The query's Shoup factors y' = floor(y*2^64/p) mod 2^64 for every word of n_ct query
-// ciphertexts ([ct][half][modulus][coefficient], the layout of the query), the values
-// PIRReplyGeneratorNFL_internal::pushQuery stores as "primes" (…NFL_internal.cpp:757-778).
-// Memory-bound: 8 bytes read and 8 written per word, 16-byte accesses.
-__global__ void __launch_bounds__(256) query_factors_kernel(const ulonglong2 *__restrict__ q,
-                                                            ulonglong2 *__restrict__ qf, uint64_t n_pairs,
-                                                            uint32_t N, uint32_t m, const DevModuli dm) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_pairs; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t c = (uint32_t)((2 * i / N) % m);  // N is even: both words share the modulus
-    const uint64_t p = dm.p[c];
-    const uint32_t delta = (uint32_t)dm.shoup_delta[c];
-    const ulonglong2 y = q[i];
-    qf[i] = make_ulonglong2(shoup_factor8(y.x, p, delta), shoup_factor8(y.y, p, delta));
-  }
-}
-
-// Tensor maps of one task for tile shape (W, C, E).
-template <int W, int C, int E>
-bool encode_task(const uint64_t *db, const uint64_t *query, const uint64_t *factors, uint64_t n_real, uint64_t P,
-                 uint64_t n_i, const ParamSet &ps, CUtensorMap *tm_db, CUtensorMap *tm_q, CUtensorMap *tm_qf) {
+// Tensor maps of one task for tile shape (W, C, E); GRP tiles load one poly column per
+// group box.
+template <int W, int C, int E, bool GRP>
+bool encode_task(const uint64_t *db, const uint64_t *query, uint64_t n_real, uint64_t P, uint64_t n_i,
+                 const ParamSet &ps, CUtensorMap *tm_db, CUtensorMap *tm_q) {
   const uint64_t N = ps.N, m = ps.m;
   const uint64_t db_dims[4] = {N, m, P, n_real};
   const uint64_t db_strides[3] = {N * 8, m * N * 8, P * m * N * 8};
-  const uint32_t db_box[4] = {(uint32_t)W, 1, (uint32_t)C, (uint32_t)E};
+  const uint32_t db_box[4] = {(uint32_t)W, 1, GRP ? 1u : (uint32_t)C, (uint32_t)E};
   const uint64_t q_dims[4] = {N, m, 2, n_i};
   const uint64_t q_strides[3] = {N * 8, m * N * 8, 2 * m * N * 8};
   const uint32_t q_box[4] = {(uint32_t)W, 1, 2, (uint32_t)E};
-  if (!encode_tensor_map_u64_4d(tm_db, db, db_dims, db_strides, db_box) ||
-      !encode_tensor_map_u64_4d(tm_q, query, q_dims, q_strides, q_box))
-    return false;
-  if (factors) return encode_tensor_map_u64_4d(tm_qf, factors, q_dims, q_strides, q_box);
-  *tm_qf = *tm_q;  // unused by tiles without precomputed factors
-  return true;
+  return encode_tensor_map_u64_4d(tm_db, db, db_dims, db_strides, db_box) &&
+         encode_tensor_map_u64_4d(tm_q, query, q_dims, q_strides, q_box);
 }
 
-template <int W, int C, int E, int NS, int TB, int IPT, bool PRE>
+template <int W, int C, int E, int NS, int TB, int IPT, bool GRP>
 cudaError_t launch_c(const ReplyLevelArgs &a, const ParamSet &ps, const DevModuli &dm, uint64_t groups,
                      cudaStream_t stream, int *status) {
-  CUtensorMap tm_db, tm_q, tm_qf;
-  if (PRE && !a.query_factors) return cudaErrorInvalidValue;
-  if (!encode_task<W, C, E>(a.db, a.query, PRE ? a.query_factors : nullptr, a.n_real, a.P, a.n_i, ps, &tm_db,
-                            &tm_q, &tm_qf))
+  CUtensorMap tm_db, tm_q;
+  if (!encode_task<W, C, E, GRP>(a.db, a.query, a.n_real, a.P, a.n_i, ps, &tm_db, &tm_q))
     return cudaErrorInvalidValue;
-  using S = Cfg<W, C, E, NS, TB, IPT, PRE>;
-  auto kern = reply_tma_kernel<W, C, E, NS, TB, IPT, PRE>;
+  using S = Cfg<W, C, E, NS, TB, IPT, GRP>;
+  auto kern = reply_tma_kernel<W, C, E, NS, TB, IPT, GRP>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kBytes);
   if (e != cudaSuccess) return e;
-  const uint32_t col_blocks = (uint32_t)((a.P + C - 1) / C);
-  LevelShape sh{a.n_real, a.P, a.n_i, ps.N, ps.m, col_blocks};
-  if (groups > 0x7fffffffull || (uint64_t)ps.m * col_blocks > 65535) return cudaErrorInvalidValue;
-  dim3 grid((unsigned)groups, (ps.N + W - 1) / W, (unsigned)(ps.m * col_blocks));
-  kern<<<grid, S::kThreads, S::kBytes, stream>>>(tm_db, tm_q, tm_qf, a.out, sh, dm, status);
+  if (GRP && (a.P != 1 || ((groups + C - 1) / C * C + 1) * a.n_i >= (1ull << 31))) return cudaErrorInvalidValue;
+  const uint32_t col_blocks = GRP ? 1 : (uint32_t)((a.P + C - 1) / C);
+  const uint64_t blocks = GRP ? (groups + C - 1) / C : groups;
+  LevelShape sh{a.n_real, a.P, a.n_i, ps.N, ps.m, col_blocks, groups};
+  if (blocks > 0x7fffffffull || (uint64_t)ps.m * col_blocks > 65535) return cudaErrorInvalidValue;
+  dim3 grid((unsigned)blocks, (ps.N + W - 1) / W, (unsigned)(ps.m * col_blocks));
+  kern<<<grid, S::kThreads, S::kBytes, stream>>>(tm_db, tm_q, a.out, sh, dm, status);
   return cudaGetLastError();
 }
 
-template <int W, int C, int E, int NS, int TB, int IPT, bool PRE>
-cudaError_t launch_tasks_c(const uint64_t *const *db, const uint64_t *const *query,
-                           const uint64_t *const *factors, uint64_t *const *out, uint32_t ntasks, uint64_t n_real,
+template <int W, int C, int E, int NS, int TB, int IPT, bool GRP>
+cudaError_t launch_tasks_c(const uint64_t *const *db, const uint64_t *const *query, uint64_t *const *out,
+                           uint32_t ntasks, uint64_t n_real,
                            uint64_t P, uint64_t groups, uint64_t n_i, const ParamSet &ps, const DevModuli &dm,
                            ReplyTask *host_tasks, ReplyTask *dev_tasks, cudaStream_t stream, int *status) {
-  if (PRE && !factors) return cudaErrorInvalidValue;
   for (uint32_t t = 0; t < ntasks; t++) {
-    if (!encode_task<W, C, E>(db[t], query[t], PRE ? factors[t] : nullptr, n_real, P, n_i, ps, &host_tasks[t].tm_db,
-                              &host_tasks[t].tm_q, &host_tasks[t].tm_qf))
+    if (!encode_task<W, C, E, GRP>(db[t], query[t], n_real, P, n_i, ps, &host_tasks[t].tm_db, &host_tasks[t].tm_q))
       return cudaErrorInvalidValue;
     host_tasks[t].out = out[t];
   }
   cudaError_t e = cudaMemcpyAsync(dev_tasks, host_tasks, ntasks * sizeof(ReplyTask), cudaMemcpyHostToDevice, stream);
   if (e != cudaSuccess) return e;
-  using S = Cfg<W, C, E, NS, TB, IPT, PRE>;
-  auto kern = reply_tma_tasks_kernel<W, C, E, NS, TB, IPT, PRE>;
+  using S = Cfg<W, C, E, NS, TB, IPT, GRP>;
+  auto kern = reply_tma_tasks_kernel<W, C, E, NS, TB, IPT, GRP>;
   e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kBytes);
   if (e != cudaSuccess) return e;
-  const uint32_t col_blocks = (uint32_t)((P + C - 1) / C);
-  LevelShape sh{n_real, P, n_i, ps.N, ps.m, col_blocks};
-  if (groups * ntasks > 0x7fffffffull || (uint64_t)ps.m * col_blocks > 65535) return cudaErrorInvalidValue;
-  dim3 grid((unsigned)(groups * ntasks), (ps.N + W - 1) / W, (unsigned)(ps.m * col_blocks));
+  if (GRP && (P != 1 || ((groups + C - 1) / C * C + 1) * n_i >= (1ull << 31))) return cudaErrorInvalidValue;
+  const uint32_t col_blocks = GRP ? 1 : (uint32_t)((P + C - 1) / C);
+  const uint64_t blocks = GRP ? (groups + C - 1) / C : groups;
+  LevelShape sh{n_real, P, n_i, ps.N, ps.m, col_blocks, groups};
+  if (blocks * ntasks > 0x7fffffffull || (uint64_t)ps.m * col_blocks > 65535) return cudaErrorInvalidValue;
+  dim3 grid((unsigned)(blocks * ntasks), (ps.N + W - 1) / W, (unsigned)(ps.m * col_blocks));
   kern<<<grid, S::kThreads, S::kBytes, stream>>>(dev_tasks, ntasks, sh, dm, status);
   return cudaGetLastError();
 }
 
 typedef cudaError_t (*SingleFn)(const ReplyLevelArgs &, const ParamSet &, const DevModuli &, uint64_t, cudaStream_t,
                                 int *);
-typedef cudaError_t (*TasksFn)(const uint64_t *const *, const uint64_t *const *, const uint64_t *const *,
-                               uint64_t *const *, uint32_t, uint64_t, uint64_t, uint64_t, uint64_t, const ParamSet &,
+typedef cudaError_t (*TasksFn)(const uint64_t *const *, const uint64_t *const *, uint64_t *const *, uint32_t, uint64_t, uint64_t, uint64_t, uint64_t, const ParamSet &,
                                const DevModuli &, ReplyTask *, ReplyTask *, cudaStream_t, int *);
 struct TileEntry {
   TileShape shape;
@@ -396,9 +377,9 @@ struct TileEntry {
   TasksFn tasks;
 };
 
-#define XPIR_TILE_P(W, C, E, NS, TB, IPT, PRE) \
-  { {W, C, E, NS, TB, IPT, PRE}, &launch_c<W, C, E, NS, TB, IPT, PRE>, &launch_tasks_c<W, C, E, NS, TB, IPT, PRE> }
-#define XPIR_TILE(W, C, E, NS, TB, IPT) XPIR_TILE_P(W, C, E, NS, TB, IPT, false)
+#define XPIR_TILE_G(W, C, E, NS, TB, IPT, GRP) \
+  { {W, C, E, NS, TB, IPT, GRP}, &launch_c<W, C, E, NS, TB, IPT, GRP>, &launch_tasks_c<W, C, E, NS, TB, IPT, GRP> }
+#define XPIR_TILE(W, C, E, NS, TB, IPT) XPIR_TILE_G(W, C, E, NS, TB, IPT, false)
 
 // Every compiled tile shape.  Entries 0..2 are the one-column shapes for grids of at
 // most two CTAs per SM, picked by slice width (two slot pairs per compute thread);
@@ -406,9 +387,10 @@ struct TileEntry {
 // warps per SM); entries 4..5 are further one-column shapes for the autotuner; then one
 // entry per column count 2..8 with 16-coefficient slices, and the same with 8 (twice
 // the CTAs, for levels whose grid would not fill the GPU).  E, NS, TB come from timing
-// sweeps on B200 over E in {16..128}, NS in {2..8}, TB in {2, 4, 8}.  The last entry
-// reads precomputed query factors: one column, for levels whose query slots are shared
-// by several groups (each factor is then derived once instead of once per group).
+// sweeps on B200 over E in {16..128}, NS in {2..8}, TB in {2, 4, 8}.  The last entries
+// take C groups as columns, for one-poly levels with several groups (the recursion's
+// first level): each query tile and Shoup factor then serves C groups, which cuts the
+// L2-to-SM query traffic and the factor work by C and puts 2*C*W chains in each CTA.
 const TileEntry kTiles[] = {
     XPIR_TILE(14, 1, 64, 3, 2, 2),
     XPIR_TILE(16, 1, 64, 3, 2, 2),
@@ -430,12 +412,17 @@ const TileEntry kTiles[] = {
     XPIR_TILE(8, 6, 32, 3, 2, 1),
     XPIR_TILE(8, 7, 32, 3, 2, 1),
     XPIR_TILE(8, 8, 32, 3, 2, 1),
-    XPIR_TILE_P(16, 1, 64, 2, 2, 1, true),
+    XPIR_TILE_G(16, 2, 32, 3, 2, 1, true),
+    XPIR_TILE_G(16, 4, 16, 3, 2, 1, true),
+    XPIR_TILE_G(16, 8, 16, 3, 2, 1, true),
+    XPIR_TILE_G(8, 4, 32, 3, 2, 1, true),
+    XPIR_TILE_G(8, 8, 32, 3, 2, 1, true),
 };
 constexpr int kTileCount = sizeof(kTiles) / sizeof(kTiles[0]);
 constexpr int kFirstColumnTile = 6;        // entry of C = 2, W = 16
 constexpr int kFirstNarrowColumnTile = 13;  // entry of C = 2, W = 8
-constexpr int kPreTile = 20;               // one column, precomputed factors
+constexpr int kFirstGroupTile = 20;        // group columns (one-poly levels)
+constexpr int kGroupTile = 21;             // default for one-poly levels with >= 4 groups: C = 4, W = 16
 constexpr int kManyCtaTile = 3;      // one column, grids beyond two CTAs per SM
 
 // Streaming multiprocessors of the current device (cached per device).
@@ -460,13 +447,17 @@ bool reply_level_supported(const ParamSet &ps, uint64_t n_real, uint64_t n_i, ui
   return ps.N % 16 == 0 && n_real < (1ull << 31) && groups * n_i + 256 < (1ull << 31);
 }
 
-// One column per CTA: every CTA of a level does the same work (its slice width W times
+// One-poly levels with at least four groups (per task) take group columns.  Otherwise
+// one column per CTA: every CTA of a level does the same work (its slice width W times
 // the level's slots), and an SM's CTAs share its issue slots, so a grid of at most two
-// CTAs per SM takes about ceil(CTAs / SMs) * W.  The default takes the slice width that minimises this (the
-// widest on ties: longer TMA rows), e.g. W=14 for N=2048 and two moduli (294 CTAs on
-// 148 SMs against 256 for W=16, which leaves 40 SMs with half the work of the others).
-int default_tile(uint64_t P, uint32_t N, uint32_t m, uint64_t ctas_per_slice) {
+// CTAs per SM takes about ceil(CTAs / SMs) * W.  The default takes the slice width that
+// minimises this (the widest on ties: longer TMA rows), e.g. W=14 for N=2048 and two
+// moduli (294 CTAs on 148 SMs against 256 for W=16, which leaves 40 SMs with half the
+// work of the others).
+int default_tile(uint64_t P, uint32_t N, uint32_t m, uint64_t groups, uint64_t ntasks) {
   const uint64_t sms = (uint64_t)sm_count();
+  const uint64_t ctas_per_slice = groups * ntasks;
+  if (P == 1 && groups >= (uint64_t)kTiles[kGroupTile].shape.C) return kGroupTile;
   if (P > 1) {
     // C columns per CTA; 16- or 8-coefficient slices by the same cost (the 1,000 x 12 KB
     // level at N=1024: 64 CTAs of W=16 against 128 of W=8, which run 1.7x faster).
@@ -497,25 +488,37 @@ int default_tile(uint64_t P, uint32_t N, uint32_t m, uint64_t ctas_per_slice) {
 }
 
 std::vector<int> tile_candidates(uint64_t P) {
-  if (P <= 1) return {0, 1, 2, 3, 4, 5};
-  // several columns per CTA (query factors shared), 16- or 8-coefficient slices, or
+  if (P <= 1) {
+    std::vector<int> c = {0, 1, 2, 3, 4, 5};
+    for (int t = kFirstGroupTile; t < kTileCount; t++) c.push_back(t);
+    return c;
+  }
+  // several columns per CTA (query tiles shared), 16- or 8-coefficient slices, or
   // one column per CTA
   const int C = (int)(P >= 8 ? 8 : P);
   return {kFirstColumnTile + C - 2, kFirstNarrowColumnTile + C - 2, kManyCtaTile};
 }
 
 TileShape tile_shape(int tile) { return kTiles[tile].shape; }
+
+// Whether a tile can run a level with P polys per element: poly columns no wider than P
+// (at most 8), group columns only for one-poly levels.
+bool tile_fits(int tile, uint64_t P) {
+  if (tile < 0 || tile >= kTileCount) return false;
+  if (kTiles[tile].shape.grp) return P == 1;
+  return kTiles[tile].shape.C <= (int)(P > 8 ? 8 : P);
+}
 int tile_count() { return kTileCount; }
 
-cudaError_t launch_reply_tasks(const uint64_t *const *db, const uint64_t *const *query,
-                               const uint64_t *const *factors, uint64_t *const *out, uint32_t ntasks, uint64_t n_real,
+cudaError_t launch_reply_tasks(const uint64_t *const *db, const uint64_t *const *query, uint64_t *const *out,
+                               uint32_t ntasks, uint64_t n_real,
                                uint64_t P, uint64_t n_groups, uint64_t n_i, const ParamSet &ps, const DevModuli &dm,
                                ReplyTask *host_tasks, ReplyTask *dev_tasks, cudaStream_t stream, uint32_t *launches,
-                               int *status, int tile) {
+                               int *status, int tile, bool write_idle) {
   if (ntasks == 0) return cudaSuccess;
   const uint64_t ct_words = 2ull * ps.m * ps.N;
   const uint64_t active = active_groups(n_real, n_i, n_groups);
-  if (active < n_groups) {
+  if (active < n_groups && write_idle) {
     for (uint32_t t = 0; t < ntasks; t++) {
       cudaError_t e = cudaMemsetAsync(out[t] + active * P * ct_words, 0,
                                       (n_groups - active) * P * ct_words * sizeof(uint64_t), stream);
@@ -524,12 +527,9 @@ cudaError_t launch_reply_tasks(const uint64_t *const *db, const uint64_t *const 
   }
   if (active == 0) return cudaSuccess;
   if (!reply_level_supported(ps, n_real, n_i, active * ntasks)) return cudaErrorNotSupported;
-  if (factors && P == 1)
-    tile = kPreTile;
-  else if (tile < 0 || tile >= kTileCount || kTiles[tile].shape.pre || kTiles[tile].shape.C > (int)(P > 8 ? 8 : P))
-    tile = default_tile(P, ps.N, ps.m, active * ntasks);
+  if (!tile_fits(tile, P)) tile = default_tile(P, ps.N, ps.m, active, ntasks);
   if (launches) (*launches)++;
-  return kTiles[tile].tasks(db, query, factors, out, ntasks, n_real, P, active, n_i, ps, dm, host_tasks, dev_tasks,
+  return kTiles[tile].tasks(db, query, out, ntasks, n_real, P, active, n_i, ps, dm, host_tasks, dev_tasks,
                             stream, status);
 }
 
@@ -539,7 +539,7 @@ cudaError_t launch_reply_level(const ReplyLevelArgs &a, const ParamSet &ps, cons
   // Groups whose every slot is past the real elements accumulate only zero terms from
   // a zero start: their replies are exactly zero.  Only groups with data are launched.
   const uint64_t active = active_groups(a.n_real, a.n_i, a.n_groups);
-  if (active < a.n_groups) {
+  if (active < a.n_groups && a.write_idle) {
     cudaError_t e = cudaMemsetAsync(a.out + active * a.P * ct_words, 0,
                                     (a.n_groups - active) * a.P * ct_words * sizeof(uint64_t), stream);
     if (e != cudaSuccess) return e;
@@ -547,22 +547,8 @@ cudaError_t launch_reply_level(const ReplyLevelArgs &a, const ParamSet &ps, cons
   if (active == 0) return cudaSuccess;
   if (!reply_level_supported(ps, a.n_real, a.n_i, active)) return cudaErrorNotSupported;
   if (launches) (*launches)++;
-  if (a.query_factors && a.P == 1)
-    tile = kPreTile;
-  else if (tile < 0 || tile >= kTileCount || kTiles[tile].shape.pre || kTiles[tile].shape.C > (int)(a.P > 8 ? 8 : a.P))
-    tile = default_tile(a.P, ps.N, ps.m, active);
+  if (!tile_fits(tile, a.P)) tile = default_tile(a.P, ps.N, ps.m, active, 1);
   return kTiles[tile].single(a, ps, dm, active, stream, status);
-}
-
-cudaError_t launch_query_factors(const uint64_t *query, uint64_t *factors, uint64_t n_ct, const ParamSet &ps,
-                                 const DevModuli &dm, cudaStream_t stream, uint32_t *launches) {
-  const uint64_t pairs = n_ct * ps.m * ps.N;  // 2*m*N words per ciphertext, two per thread
-  if (pairs == 0) return cudaSuccess;
-  const uint64_t blocks = std::min<uint64_t>((pairs + 255) / 256, (uint64_t)sm_count() * 8);
-  query_factors_kernel<<<(unsigned)blocks, 256, 0, stream>>>((const ulonglong2 *)query, (ulonglong2 *)factors, pairs,
-                                                              ps.N, ps.m, dm);
-  if (launches) (*launches)++;
-  return cudaGetLastError();
 }
 
 }  // namespace xpir

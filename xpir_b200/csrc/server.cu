@@ -106,10 +106,9 @@ void compute_batch(xpir_b200_server *srv, uint32_t lane, std::vector<xpir::Job *
     r.replies = q->dr;
     r.capacity_bytes = q->reply_bytes;
   }
-  const xpir::WorkspaceFn ws = [&](size_t a, size_t b, size_t f, void **pa, void **pb, void **pf) -> cudaError_t {
-    cudaError_t r = alloc(a, pa);
-    if (r == cudaSuccess) r = alloc(b, pb);
-    return r == cudaSuccess ? alloc(f, pf) : r;
+  const xpir::WorkspaceFn ws = [&](size_t a, size_t b, void **pa, void **pb) -> cudaError_t {
+    const cudaError_t r = alloc(a, pa);
+    return r == cudaSuccess ? alloc(b, pb) : r;
   };
   const bool run = e == cudaSuccess && upload == XPIR_B200_OK;
   if (run) xpir::reply_batch_impl(ctx, reqs.data(), (uint32_t)reqs.size(), 0, &ws);
@@ -149,18 +148,13 @@ bool footprint_of(const xpir_b200_db *db, uint32_t d, const uint32_t *n, uint64_
     nq += n[i];
   }
   if (slots < db->n_agg) return false;
-  uint64_t fws = 0, real = db->n_agg;
-  for (uint32_t lvl = 0; lvl < d; lvl++) {
+  for (uint32_t lvl = 0; lvl + 1 < d; lvl++) {
     uint64_t groups = 1;
     for (uint32_t j = lvl + 1; j < d; j++) groups *= n[j];
-    if (xpir::level_uses_factors(P, xpir::active_groups(real, n[lvl], groups))) fws = std::max(fws, n[lvl] * ct_bytes);
-    if (lvl + 1 == d) break;
     const uint64_t P2 = xpir::polys_for_bits(P * ct_bytes * 8, db->b, ctx->ps.N);
     ws = std::max(ws, groups * P * ct_bytes + groups * P2 * mN * 8);
     P = P2;
-    real = groups;
   }
-  ws += fws;
   *query_bytes = nq * ct_bytes;
   *reply_bytes = P * ct_bytes;
   *footprint = *query_bytes + *reply_bytes + ws;
