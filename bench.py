@@ -805,7 +805,8 @@ def main() -> int:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--elements", type=int, default=0,
-                    help="override the element count of a d=1 workload (profiling runs on a smaller case)")
+                    help="override the element count (profiling runs on a smaller case): a d=1 workload's "
+                         "grid follows it, a d>1 workload keeps its grid")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     w = dict(WORKLOADS[args.workload])
@@ -818,9 +819,11 @@ def main() -> int:
             return reference_batched_arm(args, w, world, rank)
         return batched_arm(args, w, world, rank, local)
     if args.elements:
-        if len(w["n"]) != 1:
-            ap.error("--elements applies to d=1 workloads")
-        w.update(F=args.elements, n=[args.elements], sample=min(w["sample"], args.elements),
+        if len(w["n"]) == 1:
+            w.update(n=[args.elements])
+        elif args.elements > math.prod(w["n"]) * w["alpha"]:
+            ap.error("--elements: more elements than the workload's grid holds")
+        w.update(F=args.elements, sample=min(w["sample"], args.elements),
                  desc=w["desc"].replace(f"{WORKLOADS[args.workload]['F']} x", f"{args.elements} x"))
     if args.impl == "reference":
         return reference_arm(args, w, world, rank)

@@ -277,10 +277,17 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
   }
 }
 
-// Two CTAs per SM for the narrow tiles (shared memory allows it), one for the wide ones.
+// Two CTAs per SM for the narrow poly-column tiles (shared memory allows it), one for the
+// wide ones; group-column tiles as many as their shared memory allows, up to three (the
+// register budget then leaves them unspilled).
 template <int W, int C, int E, int NS, int TB, int IPT, bool GRP>
 constexpr int min_blocks() {
-  return ((C <= 2 || (GRP && C <= 4)) && Cfg<W, C, E, NS, TB, IPT, GRP>::kThreads <= 640) ? 2 : 1;
+  using S = Cfg<W, C, E, NS, TB, IPT, GRP>;
+  if constexpr (GRP) {
+    constexpr size_t by_smem = (size_t)227 * 1024 / (S::kBytes + 1024);
+    return by_smem >= 3 ? 3 : (by_smem == 2 ? 2 : 1);
+  }
+  return (C <= 2 && S::kThreads <= 640) ? 2 : 1;
 }
 
 // One query: tensor maps as grid constants.  Grid: x = group (GRP: block of C groups).
