@@ -52,13 +52,16 @@ struct Cfg {
   static constexpr int kChainThreads = 2 * C * W;
   static constexpr int kChainWarps = (kChainThreads + 31) / 32;
   static constexpr int kThreads = 32 * (1 + kComputeWarps + kChainWarps);
-  static constexpr int kX = E * C * W;     // DB box    [E][C][W], with GRP [C][E][W]
-  static constexpr int kQ = E * 2 * W;     // query box [E][2][W]
+  // TMA rows start on a 32-byte sector: a slice whose start is only 16-byte aligned
+  // (W = 2 mod 4) loads a box two coefficients wider, from the sector boundary below it.
+  static constexpr int kBW = (W % 4 == 0) ? W : W + 2;
+  static constexpr int kX = E * C * kBW;   // DB box    [E][C][kBW], with GRP [C][E][kBW]
+  static constexpr int kQ = E * 2 * kBW;   // query box [E][2][kBW]
   static constexpr int kT = 2 * C * E * W;  // terms     [half][C][E/2][W][2] per buffer
   static constexpr size_t kBytes = (size_t)(NS * (kX + kQ) + TB * kT) * 8 + (2 * NS + 2 * TB) * 8;
   static_assert((TB & (TB - 1)) == 0, "term buffers: a power of two");
   static_assert(E % 2 == 0 && (E * W / 2) % (32 * IPT) == 0, "slot pairs must fill whole warps");
-  static_assert((W * 8) % 16 == 0, "TMA rows must be multiples of 16 bytes");
+  static_assert(W % 2 == 0, "TMA rows must be multiples of 16 bytes");
   static_assert(!GRP || C > 1, "group columns: at least two groups");
 };
 
@@ -104,6 +107,7 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
 
   const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int k0 = blockIdx.y * kW;
+  const int ka = k0 & ~3, off = k0 - ka;  // sector-aligned box start; the slice begins at off
   const uint32_t c = blockIdx.z / sh.col_blocks;
   const uint32_t cp0 = (blockIdx.z - c * sh.col_blocks) * C;
   const uint64_t p = dm.p[c];
@@ -145,12 +149,12 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
         if constexpr (GRP) {
 #pragma unroll
           for (int col = 0; col < C; col++)
-            tma_load_4d(xs + s * S::kX + col * E * kW, tm_db, k0, (int)c, 0, (int)((g * C + col) * sh.n_i) + slot,
-                        full + s);
+            tma_load_4d(xs + s * S::kX + col * E * S::kBW, tm_db, ka, (int)c, 0,
+                        (int)((g * C + col) * sh.n_i) + slot, full + s);
         } else {
-          tma_load_4d(xs + s * S::kX, tm_db, k0, (int)c, (int)cp0, (int)(g * sh.n_i) + slot, full + s);
+          tma_load_4d(xs + s * S::kX, tm_db, ka, (int)c, (int)cp0, (int)(g * sh.n_i) + slot, full + s);
         }
-        tma_load_4d(qs + s * S::kQ, tm_q, k0, (int)c, 0, slot, full + s);
+        tma_load_4d(qs + s * S::kQ, tm_q, ka, (int)c, 0, slot, full + s);
       }
       // Drain: every issued copy must have landed before the CTA exits.
       const uint32_t first = t > (uint32_t)NS ? t - NS : 0;
@@ -164,8 +168,8 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
       if (!mbar_wait(full + s, (t / NS) & 1)) ok = false;
       if (ok && t >= (uint32_t)TB && !mbar_wait(tempty + b, (t / TB - 1) & 1)) ok = false;
       if (!ok) break;
-      const uint64_t *xst = xs + s * S::kX;
-      const uint64_t *qst = qs + s * S::kQ;
+      const uint64_t *xst = xs + s * S::kX + off;
+      const uint64_t *qst = qs + s * S::kQ + off;
       uint64_t *tb = terms + b * S::kT;
       // Thread -> IPT items (coefficient k, slot pair e, e+1); the pair is stored as one
       // 16-byte word so that a chain thread reads two consecutive slots with one load.
@@ -178,16 +182,16 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
           const int item = ct + it * kComputeThreads;
           const int k = item % kW, ep = item / kW, e = 2 * ep;
           uint64_t x[C][2];
-          const uint64_t ya0 = qst[(e * 2 + 0) * kW + k], yb0 = qst[(e * 2 + 1) * kW + k];
-          const uint64_t ya1 = qst[(e * 2 + 2) * kW + k], yb1 = qst[(e * 2 + 3) * kW + k];
+          const uint64_t ya0 = qst[(e * 2 + 0) * S::kBW + k], yb0 = qst[(e * 2 + 1) * S::kBW + k];
+          const uint64_t ya1 = qst[(e * 2 + 2) * S::kBW + k], yb1 = qst[(e * 2 + 3) * S::kBW + k];
 #pragma unroll
           for (int col = 0; col < C; col++) {
             if constexpr (GRP) {
-              x[col][0] = xst[(col * E + e) * kW + k];
-              x[col][1] = xst[(col * E + e + 1) * kW + k];
+              x[col][0] = xst[(col * E + e) * S::kBW + k];
+              x[col][1] = xst[(col * E + e + 1) * S::kBW + k];
             } else {
-              x[col][0] = xst[(e * C + col) * kW + k];
-              x[col][1] = xst[((e + 1) * C + col) * kW + k];
+              x[col][0] = xst[(e * C + col) * S::kBW + k];
+              x[col][1] = xst[((e + 1) * C + col) * S::kBW + k];
             }
           }
           const uint64_t ysa0 = shoup_factor8_np(ya0, p, np, delta), ysb0 = shoup_factor8_np(yb0, p, np, delta);
@@ -206,11 +210,11 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
         for (int it = 0; it < IPT; it++) {
           const int item = ct + it * kComputeThreads;
           const int k = item % kW, ep = item / kW, e = 2 * ep;
-          const uint64_t ya0 = qst[(e * 2 + 0) * kW + k], yb0 = qst[(e * 2 + 1) * kW + k];
-          const uint64_t ya1 = qst[(e * 2 + 2) * kW + k], yb1 = qst[(e * 2 + 3) * kW + k];
+          const uint64_t ya0 = qst[(e * 2 + 0) * S::kBW + k], yb0 = qst[(e * 2 + 1) * S::kBW + k];
+          const uint64_t ya1 = qst[(e * 2 + 2) * S::kBW + k], yb1 = qst[(e * 2 + 3) * S::kBW + k];
           const uint64_t ysa0 = shoup_factor8_np(ya0, p, np, delta), ysb0 = shoup_factor8_np(yb0, p, np, delta);
           const uint64_t ysa1 = shoup_factor8_np(ya1, p, np, delta), ysb1 = shoup_factor8_np(yb1, p, np, delta);
-          const uint64_t x0 = xst[e * kW + k], x1 = xst[(e + 1) * kW + k];
+          const uint64_t x0 = xst[e * S::kBW + k], x1 = xst[(e + 1) * S::kBW + k];
           sts_v2(tb + (ep * kW + k) * 2, shoup_lazy_np(x0, ya0, ysa0, np), shoup_lazy_np(x1, ya1, ysa1, np));
           sts_v2(tb + (((E / 2) + ep) * kW + k) * 2, shoup_lazy_np(x0, yb0, ysb0, np), shoup_lazy_np(x1, yb1, ysb1, np));
         }
@@ -320,10 +324,11 @@ bool encode_task(const uint64_t *db, const uint64_t *query, uint64_t n_real, uin
   const uint64_t N = ps.N, m = ps.m;
   const uint64_t db_dims[4] = {N, m, P, n_real};
   const uint64_t db_strides[3] = {N * 8, m * N * 8, P * m * N * 8};
-  const uint32_t db_box[4] = {(uint32_t)W, 1, GRP ? 1u : (uint32_t)C, (uint32_t)E};
+  constexpr uint32_t kBW = (W % 4 == 0) ? W : W + 2;  // as Cfg::kBW
+  const uint32_t db_box[4] = {kBW, 1, GRP ? 1u : (uint32_t)C, (uint32_t)E};
   const uint64_t q_dims[4] = {N, m, 2, n_i};
   const uint64_t q_strides[3] = {N * 8, m * N * 8, 2 * m * N * 8};
-  const uint32_t q_box[4] = {(uint32_t)W, 1, 2, (uint32_t)E};
+  const uint32_t q_box[4] = {kBW, 1, 2, (uint32_t)E};
   return encode_tensor_map_u64_4d(tm_db, db, db_dims, db_strides, db_box) &&
          encode_tensor_map_u64_4d(tm_q, query, q_dims, q_strides, q_box);
 }
