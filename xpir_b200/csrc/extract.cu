@@ -73,15 +73,17 @@ __global__ void __launch_bounds__(256) decrypt_poly_kernel(const uint64_t *__res
     const uint64_t y = (temp < p) ? p - temp : p - temp % p;
     uint64_t z = b[i] + y;
     z -= (z >= p) ? p : 0;
-    poly[__brev(i) >> shift] = z;
+    poly[swz(__brev(i) >> shift)] = z;
   }
+  __syncthreads();
   const uint64_t *tab = tables + (uint64_t)c * kTableSlots * N;
-  ntt_lazy_smem(poly, tab + kInvOmega * N, tab + kInvOmegaShoup * N, N, log_n, p);
+  ntt_lazy_rb<3>(poly, tab + kInvOmega * N, tab + kInvOmegaShoup * N, N, log_n, p,
+                 [&](uint32_t k) { return poly[swz(k)]; });
   const uint64_t *iphi = tab + kInvPhi * N, *iphis = tab + kInvPhiShoup * N;
   uint64_t *o = res + (j * m + c) * N;
   for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {
     const uint32_t k = __brev(i) >> shift;
-    o[k] = shoup_mul(poly[i], iphi[k], iphis[k], p);
+    o[k] = shoup_mul(poly[swz(i)], iphi[k], iphis[k], p);
   }
 }
 

@@ -111,10 +111,11 @@ __global__ void __launch_bounds__(256) encrypt_kernel(const QueryGenArgs g, cons
       uint64_t z = shoup_mul(r, g.amp[c], g.amp_shoup[c], p) + (i == 0 ? ui : 0);
       z -= (z >= p) ? p : 0;
       if (z > p) z -= p;
-      poly[i] = shoup_mul(z, phi[i], phis[i], p);
+      poly[swz(i)] = shoup_mul(z, phi[i], phis[i], p);
     }
   }
-  ntt_lazy_smem(poly, tab + kOmega * N, tab + kOmegaShoup * N, N, log_n, p);
+  __syncthreads();
+  ntt_lazy_rb<3>(poly, tab + kOmega * N, tab + kOmegaShoup * N, N, log_n, p, [&](uint32_t k) { return poly[swz(k)]; });
   // uniform a: words [c*N, (c+1)*N) of the second call's stream
   uint64_t *a_out = out + (t * 2 * m + c) * N, *b_out = out + (t * 2 * m + m + c) * N;
   const uint64_t *s = sk + (uint64_t)c * N, *ss = sks + (uint64_t)c * N;
@@ -126,7 +127,7 @@ __global__ void __launch_bounds__(256) encrypt_kernel(const QueryGenArgs g, cons
       const uint32_t i = blk * 8 + k;
       uint64_t a = ((uint64_t)w[2 * k] | (uint64_t)w[2 * k + 1] << 32) & g.uniform_mask[c];
       if (a >= p) a -= p;
-      const uint64_t b = shoup_mac(poly[i], a, s[i], ss[i], p);
+      const uint64_t b = shoup_mac(poly[swz(i)], a, s[i], ss[i], p);
       a_out[i] = a % p;
       b_out[i] = b % p;
     }
