@@ -21,10 +21,29 @@ constexpr uint32_t kMinPolyDegree = 512;   // crypto/NFLParams.cpp:43
 constexpr uint32_t kMaxPolyDegree = 8192;  // crypto/NFLParams.cpp:44
 constexpr uint32_t kModulusBits = 60;      // crypto/NFLParams.cpp:31
 
-// High 64 bits of a 64x64-bit product.
+// High 64 bits of a 64x64-bit product.  On the device: the schoolbook product of 32-bit
+// halves with explicit carry chains (mad.lo/madc.hi), one instruction per product fewer
+// on B200 than the generic 64-bit high multiply (measured with ncu instruction counts;
+// identical results).
 XPIR_HD uint64_t mulhi(uint64_t a, uint64_t b) {
 #if defined(__CUDA_ARCH__)
-  return __umul64hi(a, b);
+  uint64_t r;
+  asm("{\n .reg .u32 a0, a1, b0, b1, t0, t1, t2;\n"
+      " mov.b64 {a0, a1}, %1;\n"
+      " mov.b64 {b0, b1}, %2;\n"
+      " mul.hi.u32 t0, a0, b0;\n"         // carry-in from the low product
+      " mad.lo.cc.u32 t0, a0, b1, t0;\n"
+      " madc.hi.u32 t1, a0, b1, 0;\n"
+      " mad.lo.cc.u32 t0, a1, b0, t0;\n"
+      " madc.hi.cc.u32 t1, a1, b0, t1;\n"
+      " addc.u32 t2, 0, 0;\n"
+      " mad.lo.cc.u32 t1, a1, b1, t1;\n"
+      " madc.hi.u32 t2, a1, b1, t2;\n"
+      " mov.b64 %0, {t1, t2};\n"
+      "}\n"
+      : "=l"(r)
+      : "l"(a), "l"(b));
+  return r;
 #else
   return (uint64_t)(((unsigned __int128)a * b) >> 64);
 #endif
