@@ -7,11 +7,14 @@
 // t_q = x_q*y_q - hi(x_q*y'_q)*p (mod 2^64) and y' = floor(y*2^64/p).  The expensive
 // part, t_q, does not depend on rop; only the add/compare/subtract is serial.
 //
-// One CTA owns a W-coefficient slice of one modulus, one group and C consecutive polys
-// ("columns") of the level database, and runs a warp-specialised pipeline:
+// One CTA owns a W-coefficient slice of one modulus and C "columns" of the level
+// database -- C consecutive polys of one group's elements, or (group-column tiles, for
+// one-poly levels) the poly of C consecutive groups -- and runs a warp-specialised
+// pipeline:
 //
 //   warp 0      TMA producer: per tile of E slots, one 4-D tiled load of the C DB
-//               columns and one of the query's a/b rows into an NS-stage ring
+//               columns (one per group for group columns) and one of the query's a/b
+//               rows into an NS-stage ring
 //               (mbarrier expect-tx completion; slots past the real elements come back
 //               as zeros from the TMA out-of-bounds fill, which is exactly XPIR's
 //               zero-padding element).
@@ -25,8 +28,9 @@
 // Every mbarrier wait is bounded; a wait that gives up sets the status word and the CTA
 // drains its in-flight copies and returns.
 //
-// Grid: x = group (fastest: CTAs sharing a query slice run together and hit in L2),
-//       y = coefficient slice, z = modulus * column blocks + column block.
+// Grid: x = group, or block of C groups (fastest: CTAs sharing a query slice run
+//       together and hit in L2), y = coefficient slice, z = modulus * column blocks +
+//       column block.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
