@@ -118,6 +118,20 @@ def test_short_group_aggregation_quirk(oracle):
     assert np.array_equal(g0[0:L], elems[0:L]) and np.all(g0[L:] == 0)
 
 
+@pytest.mark.parametrize("N,m,b", [(1024, 2, 40), (4096, 3, 74)])
+def test_zero_elements_import_to_one_constant_poly(oracle, N, m, b):
+    """The import of an all-zero element is one fixed poly per modulus, the same for every
+    element and poly, and not zero: the lazy butterfly maps 0 - 0 to 2p, whose Shoup
+    product is p. The recursion relies on this to broadcast the import of the idle groups'
+    (exactly zero) level replies instead of transforming each."""
+    L = 3 * N * b // 8  # three polys per element
+    imp = oracle.import_db(np.zeros(5 * L, dtype=np.uint8), 5, L, 1, b, N, m).reshape(-1, m, N)
+    assert imp.shape[0] == 5 * oracle.polys_for_bits(8 * L, b, N)
+    assert np.all(imp == imp[0])
+    p = np.array(oracle.moduli(m), dtype=np.uint64)[:, None]
+    assert np.all((imp[0] == 0) | (imp[0] == p)) and np.any(imp[0] != 0)
+
+
 def test_reference_extraction_recovers_element(ref):
     db = random_db(3, 12, 2000)
     r = ref.ref_run(1024, 1, [12], 1, db, 12, 2000, keyseed=9, chosen=7)
