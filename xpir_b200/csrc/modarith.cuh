@@ -49,16 +49,12 @@ XPIR_HD uint64_t mulhi(uint64_t a, uint64_t b) {
 #endif
 }
 
-// Shoup product without the final correction: x*y - floor(x*ys/2^64)*p (mod 2^64).
-// For ys = floor(y*2^64/p) and y < p the result lies in [0, 2p) for any 64-bit x.
-XPIR_HD uint64_t shoup_lazy(uint64_t x, uint64_t y, uint64_t ys, uint64_t p) {
-  return x * y - mulhi(x, ys) * p;
-}
-
-// The same product given np = 2^64 - p: x*y + q*np (mod 2^64), so that the second
-// product accumulates onto the first in multiply-add instructions.  Device code passes
-// np through opaque() so that the compiler keeps this form instead of rewriting it back
-// into a product and a subtraction.
+// Shoup product without the final correction, given np = 2^64 - p:
+// x*y - floor(x*ys/2^64)*p = x*y + q*np (mod 2^64), so that the second product
+// accumulates onto the first in multiply-add instructions.  For ys = floor(y*2^64/p) and
+// y < p the result lies in [0, 2p) for any 64-bit x.  Device code passes np through
+// opaque() so that the compiler keeps this form instead of rewriting it back into a
+// product and a subtraction.
 //
 // On the device the whole expression is one block of 32-bit multiply-adds (the high
 // product's carry chain, then the low 64 bits of x*y + q*np): 16 issued instructions on
@@ -95,6 +91,15 @@ XPIR_HD uint64_t shoup_lazy_np(uint64_t x, uint64_t y, uint64_t ys, uint64_t np)
   return r;
 #else
   return x * y + mulhi(x, ys) * np;
+#endif
+}
+
+// The same product given p (on the device through the multiply-add form above).
+XPIR_HD uint64_t shoup_lazy(uint64_t x, uint64_t y, uint64_t ys, uint64_t p) {
+#if defined(__CUDA_ARCH__)
+  return shoup_lazy_np(x, y, ys, 0 - p);
+#else
+  return x * y - mulhi(x, ys) * p;
 #endif
 }
 
