@@ -65,6 +65,20 @@ def test_invalid_shapes_rejected_without_gpu():
     assert xpir_b200.bits_per_coeff(1000, 1, 10) == 0
 
 
+def test_tile_table_and_pinning_arguments_without_gpu():
+    """The tile table is compiled in (one-column, poly-column and group-column shapes);
+    pinning a tile needs a context and a real level shape."""
+    import ctypes
+
+    import xpir_b200
+
+    assert xpir_b200.tile_count() >= 20
+    L = xpir_b200.lib()
+    assert L.xpir_b200_set_level_tile(None, 1, 16, 4, 0) == xpir_b200.ERR_ARG
+    assert L.xpir_b200_set_level_tile(None, 0, 16, 4, -1) == xpir_b200.ERR_ARG
+    assert L.xpir_b200_set_level_tile(ctypes.c_void_p(0), 1, 0, 4, 0) == xpir_b200.ERR_ARG
+
+
 def test_no_device_is_an_error_not_a_fallback():
     import xpir_b200
 
