@@ -404,9 +404,11 @@ struct TileEntry {
 // entry per column count 2..8 with 16-coefficient slices, and the same with 8 (twice
 // the CTAs, for levels whose grid would not fill the GPU).  E, NS, TB come from timing
 // sweeps on B200 over E in {16..128}, NS in {2..8}, TB in {2, 4, 8}.  The last entries
-// take C groups as columns, for one-poly levels with several groups (the recursion's
-// first level): each query tile and Shoup factor then serves C groups, which cuts the
-// L2-to-SM query traffic and the factor work by C and puts 2*C*W chains in each CTA.
+// but one take C groups as columns, for one-poly levels with several groups (the
+// recursion's first level): each query tile and Shoup factor then serves C groups, which
+// cuts the L2-to-SM query traffic and the factor work by C and puts 2*C*W chains in each
+// CTA.  The last is a seven-column narrow shape with 64-slot tiles for grids of at most
+// one CTA per SM.
 const TileEntry kTiles[] = {
     XPIR_TILE(14, 1, 64, 3, 2, 2),
     XPIR_TILE(16, 1, 64, 3, 2, 2),
@@ -433,6 +435,7 @@ const TileEntry kTiles[] = {
     XPIR_TILE_G(16, 8, 16, 3, 2, 1, true),
     XPIR_TILE_G(8, 4, 32, 3, 2, 1, true),
     XPIR_TILE_G(8, 8, 32, 3, 2, 1, true),
+    XPIR_TILE(8, 7, 64, 3, 2, 1),
 };
 constexpr int kTileCount = sizeof(kTiles) / sizeof(kTiles[0]);
 constexpr int kFirstColumnTile = 6;        // entry of C = 2, W = 16
@@ -440,6 +443,7 @@ constexpr int kFirstNarrowColumnTile = 13;  // entry of C = 2, W = 8
 constexpr int kFirstGroupTile = 20;        // group columns (one-poly levels)
 constexpr int kGroupTile = 21;             // default for one-poly levels with >= 4 groups: C = 4, W = 16
 constexpr int kManyCtaTile = 3;      // one column, grids beyond two CTAs per SM
+constexpr int kDeepNarrow7Tile = 25;  // C = 7, W = 8 with 64-slot tiles: twice the compute warps
 
 // Streaming multiprocessors of the current device (cached per device).
 int sm_count() {
@@ -484,7 +488,11 @@ int default_tile(uint64_t P, uint32_t N, uint32_t m, uint64_t groups, uint64_t n
     const uint64_t ctas16 = ctas_per_slice * m * ((N + 15) / 16) * col_blocks;
     const uint64_t ctas8 = ctas_per_slice * m * ((N + 7) / 8) * col_blocks;
     const uint64_t cost16 = (ctas16 + sms - 1) / sms * 16, cost8 = (ctas8 + sms - 1) / sms * 8;
-    return cost8 < cost16 ? narrow : wide;
+    if (cost8 >= cost16) return wide;
+    // A narrow seven-column grid with at most one CTA per SM: the 64-slot tile's eight
+    // compute warps (220 KB of shared memory, one CTA per SM) beat two 32-slot tiles' four
+    // (the 1,000 x 12 KB level at N=1024: 47 against 54 us).
+    return (C == 7 && ctas8 <= sms) ? kDeepNarrow7Tile : narrow;
   }
   int best = 1;
   uint64_t best_cost = ~0ull, best_ctas = 0;
@@ -506,12 +514,14 @@ int default_tile(uint64_t P, uint32_t N, uint32_t m, uint64_t groups, uint64_t n
 std::vector<int> tile_candidates(uint64_t P) {
   if (P <= 1) {
     std::vector<int> c = {0, 1, 2, 3, 4, 5};
-    for (int t = kFirstGroupTile; t < kTileCount; t++) c.push_back(t);
+    for (int t = kFirstGroupTile; t < kTileCount; t++)
+      if (kTiles[t].shape.grp) c.push_back(t);
     return c;
   }
   // several columns per CTA (query tiles shared), 16- or 8-coefficient slices, or
   // one column per CTA
   const int C = (int)(P >= 8 ? 8 : P);
+  if (C == 7) return {kFirstColumnTile + C - 2, kFirstNarrowColumnTile + C - 2, kDeepNarrow7Tile, kManyCtaTile};
   return {kFirstColumnTile + C - 2, kFirstNarrowColumnTile + C - 2, kManyCtaTile};
 }
 
