@@ -148,6 +148,19 @@ def dist_setup():
     return world, rank, local
 
 
+def max_over_ranks(dist, values: list[float], device: str) -> list[float]:
+    """The slowest rank's times: every rank passes its own and gets the maxima (one
+    collective, taken by every rank in the same order). Without a process group, the
+    values themselves."""
+    if dist is None:
+        return list(values)
+    import torch
+
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def synthetic_db(seed: int, F: int, L: int) -> np.ndarray:
     return np.random.default_rng(seed).integers(0, 256, size=F * L, dtype=np.uint8)
 
@@ -310,10 +323,7 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
     e2e_ms = e_start.elapsed_time(e_end) / e2e_steps
 
     # ---- aggregate over ranks ---------------------------------------------------------
-    if dist is not None:
-        t = torch.tensor([elapsed_ms, e2e_ms], dtype=torch.float64, device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms, e2e_ms = t.tolist()
+    elapsed_ms, e2e_ms = max_over_ranks(dist, [elapsed_ms, e2e_ms], f"cuda:{device}")
     total_db = db_bytes * world
     value = total_db * args.steps / (elapsed_ms / 1e3) / 1e9
     e2e_value = total_db / (e2e_ms / 1e3) / 1e9
@@ -460,10 +470,7 @@ def batched_arm(args, w: dict, world: int, rank: int, local: int) -> int:
     p1.record(stream)
     torch.cuda.synchronize()
     plain_ms = p0.elapsed_time(p1)
-    if dist is not None:
-        t = torch.tensor([batched_ms, plain_ms], dtype=torch.float64, device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        batched_ms, plain_ms = t.tolist()
+    batched_ms, plain_ms = max_over_ranks(dist, [batched_ms, plain_ms], f"cuda:{device}")
     value = world * nq / (batched_ms / 1e3)
     plain_qps = world * nq / (plain_ms / 1e3)
     if rank == 0:
