@@ -261,12 +261,15 @@ XPIR_B200_API int xpir_b200_server_destroy(xpir_b200_server *srv);
  * does not fit is rejected with XPIR_B200_ERR_ARG before anything is launched; a d = 1
  * query uses no scratch.
  *
- * The first call on a device looks up that device's scratch address; make that first
- * call before capturing a CUDA stream on it.  All calls share the one scratch area and it
- * keeps the previous call's contents (every word a call reads there is written by the
- * same call first): calls that overlap on the same GPU, from different threads or
- * contexts, race with each other and must be serialised by the caller.  The context
- * and the imported database are created beforehand with the allocating calls above. */
+ * The set-up happens in xpir_b200_ctx_create, which (with the context's device current)
+ * loads every engine kernel and the scratch area onto the device and looks up the scratch
+ * area's device address with cudaGetSymbolAddress, so that no call here loads a module
+ * (which would reserve device memory).  The context and the imported database are
+ * created beforehand with the allocating calls above.  All calls share the one scratch
+ * area and it keeps the previous call's contents (every word a call reads there is
+ * written by the same call first): calls that overlap on the same GPU, from different
+ * threads or contexts, race with each other and must be serialised by the caller.  The
+ * caller's current device is the same after the call as before it. */
 XPIR_B200_API int xpir_b200_reply_noalloc(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, const uint32_t *n,
                                           const void *query_dev, void *replies_dev, uint64_t capacity_bytes,
                                           uint64_t *nb_replies);

@@ -79,3 +79,30 @@ def test_autotune_keeps_replies_identical(engine, oracle):
         after = ctx.reply(db, n, q)
         assert np.array_equal(before, after)
         assert np.array_equal(after, oracle.reply(db.export(), F, 1, n, q, b, N, m))
+
+
+def test_graph_of_a_freed_database_is_not_replayed(engine):
+    """Captured batches are keyed by database identity, not by handle address: after the
+    database a graph read is freed, a new database -- here of the same device size but a
+    different shape (200 elements of 2 polys instead of 400 of 1), whose handle the heap
+    is likely to place at the freed one's address -- submitted with the same query and
+    reply buffers gets its own replies, not a replay of the old graph."""
+    torch = pytest.importorskip("torch")
+    N, m, n = 2048, 2, [400]
+    b = engine.bits_per_coeff(N, m, n[0])
+    assert engine.polys_per_element(3000, 1, b, N) == 1 and engine.polys_per_element(6000, 1, b, N) == 2
+    with engine.Context(N, m) as ctx:
+        q = random_query(41, n, N, m, engine.moduli(m))
+        qd = to_dev(torch, q)
+        out = torch.full((2 * 2 * m * N,), -1, dtype=torch.int64, device="cuda")
+        db1 = ctx.import_db(random_db(42, 400, 3000), 400, 3000, 1, b)
+        want1 = ctx.reply(db1, n, q)
+        assert ctx.reply_batch([(db1, n, qd, out)], use_graph=True) == [1]  # captured
+        assert np.array_equal(out[: want1.size].cpu().numpy().view(np.uint64), want1)
+        db1.free()
+        db2 = ctx.import_db(random_db(43, 200, 6000), 200, 6000, 1, b)
+        want2 = ctx.reply(db2, n, q)
+        out.fill_(-1)
+        assert ctx.reply_batch([(db2, n, qd, out)], use_graph=True) == [2]
+        assert np.array_equal(out.cpu().numpy().view(np.uint64), want2)
+        db2.free()

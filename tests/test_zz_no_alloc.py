@@ -9,7 +9,9 @@ area the library keeps in each GPU's global memory.
 The test calls the entry point through the C ABI and requires its replies to be
 bit-identical (integer data: no tolerance) to those of the allocating entry point,
 xpir_b200_reply, on two calls in a row (the scratch keeps the first call's contents),
-and checks that a query whose intermediate data exceeds the scratch is rejected.
+that the first recursive call on a new context changes neither the device's free memory
+nor torch's allocator, and that a query whose intermediate data exceeds the scratch is
+rejected.
 This file is named to be collected last, so that a run stopping at its first failure
 has run every other test before it.
 """
@@ -64,6 +66,36 @@ def test_noalloc_matches_allocating_reply(engine, oracle, N, m, n, alpha, F, L):
             assert count * 2 * m * N == want.size
             got = out_dev.cpu().numpy().view(np.uint64)
             assert np.array_equal(got, want), f"call {call}"
+        db.free()
+
+
+def test_noalloc_first_call_allocates_nothing(engine, oracle):
+    """The first d = 2 call on a fresh context: the context's creation has already loaded
+    the engine's kernels and the scratch area onto the device, so the call leaves the
+    device's free memory (cudaMemGetInfo) and torch's allocator statistics unchanged."""
+    torch = pytest.importorskip("torch")
+    N, m, n, F, L = 1024, 2, [16, 12], 150, 2000
+    b = oracle.bits_per_coeff(N, m, n[0])
+    q = random_query(77, n, N, m, engine.moduli(m))
+    with engine.Context(N, m) as ctx:
+        db = ctx.import_db(random_db(76, F, L), F, L, 1, b)
+        q_dev = torch.from_numpy(q.view(np.int64)).cuda()
+        out_dev = torch.full((2 * m * N,), -1, dtype=torch.int64, device="cuda")
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        free_before, _ = torch.cuda.mem_get_info()
+        stats_before = torch.cuda.memory_stats()
+        status, count = reply_noalloc(engine, ctx, db, n, q_dev, out_dev)
+        assert status == engine.OK, engine.lib().xpir_b200_strerror(status)
+        torch.cuda.synchronize()
+        free_after, _ = torch.cuda.mem_get_info()
+        stats_after = torch.cuda.memory_stats()
+        assert free_after == free_before
+        for key in ("allocation.all.allocated", "reserved_bytes.all.current", "allocated_bytes.all.current"):
+            assert stats_after.get(key) == stats_before.get(key), key
+        want = ctx.reply(db, n, q)
+        assert count * 2 * m * N == want.size
+        assert np.array_equal(out_dev.cpu().numpy().view(np.uint64), want)
         db.free()
 
 

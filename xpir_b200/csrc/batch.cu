@@ -140,6 +140,7 @@ cudaError_t enqueue(xpir_b200_ctx *ctx, const std::vector<Group> &groups, const 
 // whatever else the context does.
 struct BatchPlan {
   std::vector<uint64_t> key;
+  std::vector<uint64_t> db_ids;  // databases the graph reads
   uint64_t launches = 0;  // engine kernels in the captured graph
   void *ws_a = nullptr, *ws_b = nullptr, *dev_tasks = nullptr, *host_tasks = nullptr;
   cudaGraph_t graph = nullptr;
@@ -160,7 +161,7 @@ std::vector<uint64_t> plan_key(const xpir_b200_ctx *ctx, const xpir_b200_request
                                uint64_t tune_epoch) {
   std::vector<uint64_t> key{tune_epoch, (uint64_t)(uintptr_t)ctx, count};
   for (uint32_t i = 0; i < count; i++) {
-    key.push_back((uint64_t)(uintptr_t)reqs[i].db);
+    key.push_back(reqs[i].db ? reqs[i].db->id : 0);
     key.push_back(reqs[i].d);
     for (uint32_t j = 0; j < reqs[i].d && j < XPIR_B200_MAX_LEVELS; j++) key.push_back(reqs[i].n[j]);
     key.push_back((uint64_t)(uintptr_t)reqs[i].query);
@@ -172,6 +173,15 @@ std::vector<uint64_t> plan_key(const xpir_b200_ctx *ctx, const xpir_b200_request
 constexpr size_t kMaxPlans = 8;
 
 }  // namespace
+
+void xpir::drop_plans_of(xpir_b200_ctx *ctx, uint64_t db_id) {
+  auto &plans = ctx->plans;
+  plans.erase(std::remove_if(plans.begin(), plans.end(),
+                             [db_id](const std::shared_ptr<BatchPlan> &pl) {
+                               return std::find(pl->db_ids.begin(), pl->db_ids.end(), db_id) != pl->db_ids.end();
+                             }),
+              plans.end());
+}
 
 int xpir::reply_batch_impl(xpir_b200_ctx *ctx, xpir_b200_request *reqs, uint32_t count, int use_graph,
                            const WorkspaceFn *workspace) {
@@ -280,6 +290,7 @@ int xpir::reply_batch_impl(xpir_b200_ctx *ctx, xpir_b200_request *reqs, uint32_t
     }
   auto plan = std::make_shared<BatchPlan>();
   plan->key = key;
+  for (const Group &g : groups) plan->db_ids.push_back(g.db->id);
   e = cudaMalloc(&plan->ws_a, std::max<size_t>(z.ws_a, 256));
   if (e == cudaSuccess) e = cudaMalloc(&plan->ws_b, std::max<size_t>(z.ws_b, 256));
   if (e == cudaSuccess) e = cudaMalloc(&plan->dev_tasks, z.tasks * sizeof(ReplyTask));

@@ -131,6 +131,11 @@ int xpir_b200_ctx_create(xpir_b200_ctx **out, int device, uint32_t N, uint32_t m
     return XPIR_B200_ERR_ARG;
   }
   int rc = cuda_status(cudaSetDevice(device));
+  // Load every engine kernel and place the no-allocation scratch on this device now, so
+  // that no later call loads a module (module loading reserves device memory).
+  if (rc == XPIR_B200_OK) rc = cuda_status(preload_import_kernels());
+  if (rc == XPIR_B200_OK) rc = cuda_status(preload_reply_kernels());
+  if (rc == XPIR_B200_OK) rc = cuda_status(prepare_noalloc_scratch(device));
   if (rc == XPIR_B200_OK) rc = cuda_status(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
   if (rc == XPIR_B200_OK) rc = cuda_status(cudaMalloc(&ctx->d_tables, tables.size() * sizeof(uint64_t)));
   if (rc == XPIR_B200_OK)
@@ -210,6 +215,7 @@ int xpir_b200_db_import(xpir_b200_ctx *ctx, const void *elements, uint64_t nb_el
   auto *db = new (std::nothrow) xpir_b200_db();
   if (!db) return XPIR_B200_ERR_NOMEM;
   db->ctx = ctx;
+  db->id = next_db_id();
   db->n_agg = groups;
   db->P = P;
   db->b = b;
@@ -254,6 +260,7 @@ int xpir_b200_db_free(xpir_b200_db *db) {
   if (!ctx->dbs.erase(db)) return XPIR_B200_ERR_ARG;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  drop_plans_of(ctx, db->id);
   cudaFree(db->d_polys);
   delete db;
   return XPIR_B200_OK;

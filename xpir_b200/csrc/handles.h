@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <functional>
 #include <map>
 #include <memory>
@@ -53,6 +54,7 @@ inline int tuned_tile(const xpir_b200_ctx *ctx, uint64_t P, uint64_t n_i, uint64
 
 struct xpir_b200_db {
   xpir_b200_ctx *ctx = nullptr;
+  uint64_t id = 0;  // unique per import in this process (never reused, unlike the address)
   uint64_t *d_polys = nullptr;
   uint64_t n_agg = 0;
   uint64_t P = 0;
@@ -64,6 +66,17 @@ struct xpir_b200_db {
 struct xpir_b200_request;
 
 namespace xpir {
+
+// A fresh database id (1, 2, ...): captured batches are keyed by it, so a database
+// imported at the address of a freed one never replays the freed one's graph.
+inline uint64_t next_db_id() {
+  static std::atomic<uint64_t> counter{0};
+  return ++counter;
+}
+
+// Drops the captured batches that read database `db_id` (batch.cu).  The caller holds
+// ctx->mu and has synchronised the context's stream.
+void drop_plans_of(xpir_b200_ctx *ctx, uint64_t db_id);
 
 // Supplies the workspace of an uncaptured batch: device buffers of at least `a` bytes
 // (level replies) and `b` bytes (re-imported level databases), valid in stream order on

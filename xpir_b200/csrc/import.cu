@@ -233,4 +233,13 @@ cudaError_t launch_import(const AggSource &src, uint64_t groups, uint64_t P, con
   return cudaSuccess;
 }
 
+// Loads both import kernels on the current device (lazy module loading would otherwise do
+// it, and reserve their device memory, at their first launch).
+cudaError_t preload_import_kernels() {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, import_kernel);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, import_zero_fill_kernel);
+  return e;
+}
+
 }  // namespace xpir

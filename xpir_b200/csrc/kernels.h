@@ -123,4 +123,12 @@ inline uint64_t active_groups(uint64_t n_real, uint64_t n_i, uint64_t n_groups) 
 // path, degree a multiple of 16, 32-bit TMA coordinates).
 bool reply_level_supported(const ParamSet &ps, uint64_t n_real, uint64_t n_i, uint64_t groups);
 
+// Load the import and reply kernels on the current device, so that no later launch
+// loads a module (which reserves device memory).
+cudaError_t preload_import_kernels();
+cudaError_t preload_reply_kernels();
+// Places the scratch array of xpir_b200_reply_noalloc on the current device (loading
+// the module that holds it) and caches its device address (noalloc.cu).
+cudaError_t prepare_noalloc_scratch(int device);
+
 }  // namespace xpir

@@ -391,10 +391,15 @@ struct TileEntry {
   TileShape shape;
   SingleFn single;
   TasksFn tasks;
+  const void *single_kernel, *tasks_kernel;
 };
 
-#define XPIR_TILE_G(W, C, E, NS, TB, IPT, GRP) \
-  { {W, C, E, NS, TB, IPT, GRP}, &launch_c<W, C, E, NS, TB, IPT, GRP>, &launch_tasks_c<W, C, E, NS, TB, IPT, GRP> }
+#define XPIR_TILE_G(W, C, E, NS, TB, IPT, GRP)                                                              \
+  {                                                                                                        \
+    {W, C, E, NS, TB, IPT, GRP}, &launch_c<W, C, E, NS, TB, IPT, GRP>, &launch_tasks_c<W, C, E, NS, TB, IPT, GRP>, \
+        (const void *)&reply_tma_kernel<W, C, E, NS, TB, IPT, GRP>,                                          \
+        (const void *)&reply_tma_tasks_kernel<W, C, E, NS, TB, IPT, GRP>                                     \
+  }
 #define XPIR_TILE(W, C, E, NS, TB, IPT) XPIR_TILE_G(W, C, E, NS, TB, IPT, false)
 
 // Every compiled tile shape.  Entries 0..2 are the one-column shapes for grids of at
@@ -575,6 +580,18 @@ cudaError_t launch_reply_level(const ReplyLevelArgs &a, const ParamSet &ps, cons
   if (launches) (*launches)++;
   if (!tile_fits(tile, a.P)) tile = default_tile(a.P, ps.N, ps.m, active, 1);
   return kTiles[tile].single(a, ps, dm, active, stream, status);
+}
+
+// Loads every compiled reply kernel on the current device (lazy module loading would
+// otherwise do it, and reserve their device memory, at each one's first launch).
+cudaError_t preload_reply_kernels() {
+  cudaFuncAttributes fa;
+  for (const TileEntry &t : kTiles) {
+    cudaError_t e = cudaFuncGetAttributes(&fa, t.single_kernel);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, t.tasks_kernel);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace xpir
