@@ -29,12 +29,14 @@ _lib = None
 
 
 def build(reference_root: str | None = None) -> None:
-    """Compile liboracle.so, and the reference checker when its sources are present."""
+    """Compile liboracle.so, and the reference checker when the XPIR source tree is given
+    (``reference_root`` or the XPIR_REF environment variable) and present."""
     env = dict(os.environ, CC="gcc", CXX="g++")
     subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so"], check=True, env=env)
-    ref = reference_root or "/root/reference"
-    if Path(ref, "crypto", "NFLlib.cpp").exists():
-        subprocess.run(["make", "-s", "-j8", "-C", str(HERE), "ref", f"REF={ref}"], check=True, env=env)
+    ref = reference_root or os.environ.get("XPIR_REF", "")
+    if ref and Path(ref, "crypto", "NFLlib.cpp").exists():
+        subprocess.run(["make", "-s", "-j8", "-C", str(HERE), "ref", "simplepir", f"XPIR_REF={ref}"], check=True,
+                       env=env)
 
 
 def lib():

@@ -67,6 +67,17 @@ def build_pir(force: bool = False) -> Path:
     return PIR_LIB
 
 
+def build_xpir(xpir_ref: str) -> Path:
+    """XPIR's pir library with the B200 engine plugged in (xpir_b200/xpir/Makefile):
+    XPIR's sources from `xpir_ref` with libpir.cpp and PIRReplyGeneratorFactory.cpp
+    replaced by the B200 ones, archived as xpir_b200/xpir/_build/libpir_b200.a."""
+    res = subprocess.run(["make", "-s", "-j8", "-C", str(PKG / "xpir"), f"XPIR_REF={xpir_ref}"], capture_output=True,
+                         text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"building the XPIR binding failed:\n{res.stdout}\n{res.stderr}")
+    return PKG / "xpir" / "_build" / "libpir_b200.a"
+
+
 if __name__ == "__main__":
     verbose = "-v" in sys.argv
     extra = ["-Xptxas", "-v"] if "--ptxas" in sys.argv else None

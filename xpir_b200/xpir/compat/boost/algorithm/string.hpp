@@ -1,5 +1,5 @@
 // Minimal stand-in for boost::algorithm::split / is_any_of, enough for the XPIR
-// reference sources that parse "LWE:k:N:logq" descriptors.  Test infrastructure only.
+// reference sources that parse "LWE:k:N:logq" descriptors.
 #ifndef XPIR_REF_SHIM_BOOST_ALGORITHM_STRING_HPP
 #define XPIR_REF_SHIM_BOOST_ALGORITHM_STRING_HPP
 

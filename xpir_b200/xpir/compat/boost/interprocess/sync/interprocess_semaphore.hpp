@@ -1,5 +1,5 @@
 // Minimal pthread-based stand-in for boost::interprocess::interprocess_semaphore, as
-// used by XPIR's shared_queue.  Test infrastructure only.
+// used by XPIR's shared_queue.
 #ifndef XPIR_REF_SHIM_INTERPROCESS_SEMAPHORE_HPP
 #define XPIR_REF_SHIM_INTERPROCESS_SEMAPHORE_HPP
 

@@ -1,4 +1,4 @@
-// Minimal stand-in for boost::queue (boost/pending/queue.hpp).  Test infrastructure only.
+// Minimal stand-in for boost::queue (boost/pending/queue.hpp).
 #ifndef XPIR_REF_SHIM_PENDING_QUEUE_HPP
 #define XPIR_REF_SHIM_PENDING_QUEUE_HPP
 

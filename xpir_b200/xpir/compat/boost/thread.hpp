@@ -1,5 +1,5 @@
 // Minimal pthread-based stand-in for the boost::thread / boost::mutex subset that the
-// XPIR reference sources use.  Test infrastructure only.  It deliberately avoids
+// XPIR reference sources use.  It deliberately avoids
 // <thread> and <mutex>: the reference headers say "using namespace std; using namespace
 // boost;" and then name `thread` unqualified, so std::thread must not be visible.
 #ifndef XPIR_REF_SHIM_BOOST_THREAD_HPP

@@ -1,8 +1,9 @@
 /* Declarations of the public GMP 6 mpz API used by the XPIR reference sources.
  *
- * Test infrastructure only: this header lets the reference's own sources (compiled
- * unchanged as the parity checker) link against the GMP runtime library that the
- * image ships as libgmp.so.10 without development headers.  Only documented public
+ * This header lets XPIR's own sources -- compiled unchanged, both as the parity checker
+ * and with the B200 reply generator plugged in -- link against the GMP runtime library
+ * that this image ships as libgmp.so.10 without development headers.  A normal XPIR
+ * build uses the system's gmp.h instead.  Only documented public
  * types and functions are declared, under their exported __gmp names. */
 #ifndef XPIR_REF_SHIM_GMP_H
 #define XPIR_REF_SHIM_GMP_H
