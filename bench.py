@@ -39,9 +39,16 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "reply-gen DB GB/s vs HBM peak; batched vs plain queries/s; p50/p99 latency"
 
+# dram__bytes_read.sum + dram__bytes_write.sum over the algorithmic bytes (DB + query +
+# reply) of one reply_tma_kernel launch on the memory-bound workload, from one
+# `ncu --set full` capture of a 10,000-element case of the same kernel and grid
+# (traffic grows with the elements: each is one DB row and one query ciphertext):
+# (999.2 + 3.5) MB / 983.1 MB.
+REPLY_TRAFFIC_PER_ALGORITHMIC_BYTE = 1.0199
+
 WORKLOADS = {
     # name: N, m, n levels, alpha, elements, element bytes, chosen index, cpu-sample elements
-    "memory_bound": dict(N=2048, m=2, n=[100000], alpha=1, F=100000, L=4096, chosen=54321, sample=20000,
+    "memory_bound": dict(N=2048, m=2, n=[100000], alpha=1, F=100000, L=4096, chosen=54321, sample=100000,
                          desc="memory-bound single query: LWE:80:2048:120, d=1, alpha=1, 100000 x 4 KB"),
     "plain": dict(N=1024, m=1, n=[1000], alpha=1, F=1000, L=12288, chosen=137, sample=1000,
                   desc="plain single query: LWE:80:1024:60, d=1, alpha=1, 1000 x 12 KB"),
@@ -175,7 +182,11 @@ def synthetic_query(seed: int, n: list[int], N: int, m: int, moduli: list[int], 
 
 
 def run_reference(w: dict, steps: int, warmup: int, threads: int) -> dict:
-    """The XPIR reference (oracle/_ref) on a bounded sample of the workload."""
+    """The XPIR reference (oracle/_ref) answering `steps` queries after `warmup` untimed
+    ones, on one import of the workload: the full workload, except where the reference's
+    host memory for the zero-padding slots of the index grid rules it out (the recursive
+    workload: about 103 GB), where it takes `sample` elements on the same grid shape and
+    the reply time is scaled to the full database."""
     from oracle import pyoracle as po
 
     if not po.ref_available():
@@ -185,19 +196,18 @@ def run_reference(w: dict, steps: int, warmup: int, threads: int) -> dict:
     if len(n) == 1:
         n = [-(-S // w["alpha"])]
     db = synthetic_db(1, S, w["L"])
-    runs = []
-    for i in range(warmup + steps):
-        r = po.ref_run(w["N"], w["m"], n, w["alpha"], db, S, w["L"], keyseed=1000 + i, chosen=0, extract=False,
-                       threads=threads)
-        if i >= warmup:
-            runs.append(r)
-    imported = runs[0]["nb_elements"] * runs[0]["polys_per_element"] * w["m"] * w["N"] * 8
-    reply_s = [r["reply_s"] for r in runs]
-    import_s = [r["import_s"] for r in runs]
-    return {"value": imported / statistics.mean(reply_s) / 1e9, "reply_s": statistics.mean(reply_s),
-            "import_s": statistics.mean(import_s), "import_gbs": imported / statistics.mean(import_s) / 1e9,
-            "imported_bytes": imported, "elements": S, "n": n, "threads": runs[0]["omp_threads"],
-            "bits_per_coeff": runs[0]["bits_per_coeff"], "polys_per_element": runs[0]["polys_per_element"]}
+    chosen = w["chosen"] // w["alpha"] if w["chosen"] < S else 0
+    r = po.ref_bench(w["N"], w["m"], n, w["alpha"], db, S, w["L"], keyseed=1000, chosen=chosen, reps=steps,
+                     warmup=warmup, threads=threads)
+    imported = r["nb_elements"] * r["polys_per_element"] * w["m"] * w["N"] * 8
+    reply_s = statistics.mean(r["reply_s"])
+    full_imported = imported * w["F"] / S
+    full_reply_s = reply_s * w["F"] / S
+    return {"value": full_imported / full_reply_s / 1e9, "reply_s": reply_s, "full_reply_s": full_reply_s,
+            "reply_s_all": r["reply_s"], "import_s": r["import_s"], "import_gbs": imported / r["import_s"] / 1e9,
+            "imported_bytes": imported, "elements": S, "same_config": S == w["F"], "n": n,
+            "threads": r["omp_threads"], "bits_per_coeff": r["bits_per_coeff"],
+            "polys_per_element": r["polys_per_element"], "cpu_model": po.host_cpu_model()}
 
 
 def reference_arm(args, w: dict, world: int, rank: int) -> int:
@@ -208,18 +218,20 @@ def reference_arm(args, w: dict, world: int, rank: int) -> int:
     if "unavailable" in r:
         print(json.dumps({"impl": "reference", "unavailable": r["unavailable"]}))
         return 0
-    sample = (f"{r['elements']} elements of the workload (n={r['n']}, bits/coeff {r['bits_per_coeff']}), "
-              f"reply timed with omp_get_wtime boundaries as the reference prints them")
+    sample = (f"{'the full workload' if r['same_config'] else str(r['elements']) + ' elements (scaled)'} "
+              f"(n={r['n']}, bits/coeff {r['bits_per_coeff']}): one import, {args.steps} timed replies after "
+              f"{args.warmup} untimed, each timed with omp_get_wtime at the reference's own boundaries")
     line = {
         "impl": "reference", "metric": METRIC, "value": round(r["value"], 4), "unit": "GB/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(r["reply_s"] * 1e3, 3),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(r["full_reply_s"] * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
         "data": "synthetic: seeded uniform DB bytes; query from the reference's own PIRQueryGenerator",
-        "config": {"workload": w["desc"], "elements_sampled": r["elements"]},
+        "config": {"workload": w["desc"], "elements_timed": r["elements"], "same_config": r["same_config"]},
         "cpu_baseline": {"value": round(r["value"], 4), "unit": "GB/s", "cores": threads, "kind": "reference",
-                         "sample": sample},
+                         "cpu_model": r["cpu_model"], "sample": sample},
         "e2e": {"value": round(r["value"], 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "import": {"seconds": round(r["import_s"], 4), "gbs": round(r["import_gbs"], 4)},
+        "reply_s": [round(x, 4) for x in r["reply_s_all"]],
         "note": "the reference reply loop is OpenMP-parallel only over the polys of an element "
                 "(PIRReplyGeneratorNFL_internal.cpp:531-534); with 1 poly per element it runs on one thread",
     }
@@ -232,14 +244,7 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
 
     import xpir_b200
 
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dist = init_dist(world, local)
     device = local
     torch.cuda.set_device(device)
     N, m, n, alpha, F, L = w["N"], w["m"], w["n"], w["alpha"], w["F"], w["L"]
@@ -328,6 +333,7 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
     value = total_db * args.steps / (elapsed_ms / 1e3) / 1e9
     e2e_value = total_db / (e2e_ms / 1e3) / 1e9
 
+    line = None
     if rank == 0:
         peaks = measured_peaks()
         query_bytes = nq * ct_words * 8
@@ -337,12 +343,11 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
         roofline = None
         if algo_bytes:
             achieved = algo_bytes / (kern_ms / 1e3) / 1e9
-            traffic = None
-            tf = ROOT / "profiles" / "reply_level_memory_bound.md"
-            if args.workload == "memory_bound" and not args.elements and tf.exists():
-                for line in tf.read_text().splitlines():
-                    if line.strip().startswith("traffic_bytes_per_launch"):
-                        traffic = int(line.split("=")[1])
+            # DRAM traffic cannot be read without a profiler: it is the ncu capture's
+            # measured bytes per algorithmic byte of this kernel on this workload, applied
+            # to this launch's algorithmic bytes.
+            traffic = (round(algo_bytes * REPLY_TRAFFIC_PER_ALGORITHMIC_BYTE)
+                       if args.workload == "memory_bound" else None)
             roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                         "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
                         "kernel": "reply_tma_kernel", "peak_source": peaks["source"],
@@ -351,9 +356,11 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
         if world == 1 and not args.no_cpu_baseline:
             r = run_reference(w, steps=1, warmup=0, threads=os.cpu_count() or 1)
             if "unavailable" not in r:
+                what = "the full workload" if r["same_config"] else f"{r['elements']} of {F} elements (scaled)"
                 cpu = {"value": round(r["value"], 4), "unit": "GB/s", "cores": r["threads"], "kind": "reference",
-                       "sample": f"{r['elements']} of {F} elements (n={r['n']}); reference reply time "
-                                 f"{r['reply_s']:.3f} s, import {r['import_s']:.3f} s",
+                       "cpu_model": r["cpu_model"],
+                       "sample": (f"{what} (n={r['n']}); one reference reply {r['reply_s']:.3f} s, import "
+                                  f"{r['import_s']:.3f} s"),
                        "import_gbs": round(r["import_gbs"], 4)}
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
@@ -375,30 +382,68 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
             "import": {"seconds_wall": round(import_s, 4), "input_bytes": F * L, "imported_bytes": db_bytes},
             "total_gbs": round((db_bytes + nq * ct_words * 8) * world * args.steps / (elapsed_ms / 1e3) / 1e9, 2),
         }
-        print(json.dumps(line), flush=True)
     dbh.free()
     ctx.close()
+    del q_dev, q_host, out_dev, out_host, flush_buf
+    torch.cuda.empty_cache()
+    # The rest of the metric, on the same GPU after the single query's buffers are freed:
+    # batched vs plain queries/s (every rank, as replicas) and the serving loop's p50/p99
+    # latency (one GPU: a server answers on the GPU it runs on).
+    if args.extras and args.workload == "memory_bound" and not args.elements:
+        b = measure_batched(args, WORKLOADS["batched"], world, rank, local, dist)
+        if rank == 0:
+            line["batched"] = sub_object(b)
+        if world == 1:
+            line["serving"] = sub_object(measure_serving(args, WORKLOADS["serving"], local))
+        elif rank == 0:
+            line["serving"] = {"skipped": "the serving loop runs on one GPU; it is measured in the N=1 run"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
     return 0
 
 
+def sub_object(line: dict) -> dict:
+    """A workload's result line as a sub-object of the default line: without the keys
+    that repeat the enclosing line's."""
+    drop = {"metric", "n_gpus", "higher_is_better", "scaling", "vs_baseline", "dtype"}
+    return {k: v for k, v in line.items() if k not in drop}
+
+
+def init_dist(world: int, local: int):
+    """The process group of a multi-GPU run (NCCL; used for barriers and the max over
+    ranks only), or None on one GPU."""
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
 def batched_arm(args, w: dict, world: int, rank: int, local: int) -> int:
+    dist = init_dist(world, local)
+    line = measure_batched(args, w, world, rank, local, dist)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def measure_batched(args, w: dict, world: int, rank: int, local: int, dist) -> dict | None:
     """64 concurrent queries of uneven shape: one batched submission (captured in a CUDA
     graph) against 64 sequential single-query replies, both with queries resident in HBM.
-    value = queries/s of the batched form."""
+    value = queries/s of the batched form.  Returns the result line on rank 0."""
     import torch
 
     import xpir_b200
 
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     device = local
     torch.cuda.set_device(device)
     N, m, F, L = w["N"], w["m"], w["F"], w["L"]
@@ -480,14 +525,13 @@ def batched_arm(args, w: dict, world: int, rank: int, local: int) -> int:
         achieved = batch_bytes / (batched_ms / 1e3) / 1e9
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            r = run_reference(dict(WORKLOADS["memory_bound"], N=N, m=m, n=[w["sample"]], alpha=1, F=w["sample"],
-                                   L=L, sample=w["sample"]), steps=1, warmup=0, threads=os.cpu_count() or 1)
+            r = reference_batch_rate(w, os.cpu_count() or 1)
             if "unavailable" not in r:
-                full_s = r["reply_s"] * F / r["elements"]
-                cpu = {"value": round(1.0 / full_s, 4), "unit": "queries/s", "cores": r["threads"],
-                       "kind": "reference",
-                       "sample": f"one d=1/alpha=1 query on {r['elements']} of the {F} elements "
-                                 f"({r['reply_s']:.3f} s), scaled to the full database"}
+                cpu = {"value": round(r["qps"], 4), "unit": "queries/s", "cores": r["threads"], "kind": "reference",
+                       "cpu_model": r["cpu_model"],
+                       "sample": "one query of each class on the full database, the batch's time = the classes' "
+                                 "counts x their reply times (the reference answers one query at a time)",
+                       "per_class": r["per_class"]}
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "queries/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(batched_ms, 3), "higher_is_better": True, "scaling": "weak",
@@ -509,36 +553,61 @@ def batched_arm(args, w: dict, world: int, rank: int, local: int) -> int:
                         "measured on the single-query workloads",
             "gpu_launches": launches, "clocks": clocks,
         }
-        print(json.dumps(line), flush=True)
+    else:
+        line = None
+    items.clear()
     for d in dbs.values():
         d.free()
     ctx.close()
-    if dist is not None:
-        dist.destroy_process_group()
-    return 0
+    torch.cuda.empty_cache()
+    return line
+
+
+def reference_batch_rate(w: dict, threads: int) -> dict:
+    """The reference answering the batch's queries one at a time on the full database: one
+    query of each class timed (xpir_ref bench, one repetition); the batch takes the sum of
+    the classes' counts times their reply times."""
+    from oracle import pyoracle as po
+
+    if not po.ref_available():
+        return {"unavailable": "reference checker oracle/_ref/xpir_ref was not built"}
+    db = synthetic_db(4, w["F"], w["L"])
+    per, total, nq, threads_used = [], 0.0, 0, threads
+    for k, (count, n, alpha) in enumerate(w["classes"]):
+        r = po.ref_bench(w["N"], w["m"], n, alpha, db, w["F"], w["L"], keyseed=3000 + k, chosen=0, reps=1,
+                         threads=threads)
+        t = r["reply_s"][0]
+        per.append({"class": f"{count} x d={len(n)} alpha={alpha} n={n}", "reply_s": round(t, 4),
+                    "import_s": round(r["import_s"], 3)})
+        total += count * t
+        nq += count
+        threads_used = r["omp_threads"]
+    return {"qps": nq / total, "batch_s": total, "per_class": per, "threads": threads_used,
+            "cpu_model": po.host_cpu_model()}
 
 
 def reference_batched_arm(args, w: dict, world: int, rank: int) -> int:
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    S = w["sample"]
-    base = dict(WORKLOADS["memory_bound"], N=w["N"], m=w["m"], n=[S], alpha=1, F=S, L=w["L"], sample=S)
-    r = run_reference(base, args.steps, args.warmup, threads)
+    r = reference_batch_rate(w, threads)
     if "unavailable" in r:
         print(json.dumps({"impl": "reference", "unavailable": r["unavailable"]}))
         return 0
-    qps = 1.0 / (r["reply_s"] * w["F"] / r["elements"])
+    qps = r["qps"]
     line = {"impl": "reference", "metric": METRIC, "value": round(qps, 4), "unit": "queries/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 / qps, 3), "higher_is_better": True,
+            "steps": 1, "warmup": 0, "ms_per_step": round(r["batch_s"] * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64",
             "data": "synthetic: seeded uniform DB bytes; query from the reference's own PIRQueryGenerator",
             "config": {"workload": w["desc"]},
-            "cpu_baseline": {"value": round(qps, 4), "unit": "queries/s", "cores": threads, "kind": "reference",
-                             "sample": f"d=1/alpha=1 query on {r['elements']} of {w['F']} elements, scaled"},
+            "cpu_baseline": {"value": round(qps, 4), "unit": "queries/s", "cores": r["threads"], "kind": "reference",
+                             "cpu_model": r["cpu_model"],
+                             "sample": "one query of each class on the full database, scaled by the class counts",
+                             "per_class": r["per_class"]},
             "e2e": {"value": round(qps, 4), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
+
 
 def dim_sizes(n: int, alpha: int, d: int) -> list[int]:
     """Grid of a d-dimensional query over n elements aggregated by alpha: the client
@@ -594,10 +663,23 @@ def reference_mix(w: dict, threads: int) -> dict:
 
 
 def serving_arm(args, w: dict, world: int, rank: int, local: int) -> int:
+    if world > 1 and rank != 0:
+        # Replicas only: every rank would run the same independent server; the serving
+        # measurement is taken on rank 0's GPU.
+        return 0
+    line = measure_serving(args, w, local)
+    print(json.dumps(line), flush=True)
+    if not line["bit_exact"]:
+        log("some served replies differ from the replies computed alone")
+        return 1
+    return 0
+
+
+def measure_serving(args, w: dict, local: int) -> dict:
     """Poisson arrivals of mixed queries through the serving loop (xpir_b200.Server): host
     queries in, host replies out, admission by a device budget, continuous batching per
     lane.  value = completed queries/s at the highest offered rate; every reply is checked
-    against the same query's reply computed alone."""
+    against the same query's reply computed alone.  Returns the result line."""
     import queue
     import threading
 
@@ -605,10 +687,6 @@ def serving_arm(args, w: dict, world: int, rank: int, local: int) -> int:
 
     import xpir_b200
 
-    if world > 1 and rank != 0:
-        # Replicas only: every rank would run the same independent server; the serving
-        # measurement is taken on rank 0's GPU.
-        return 0
     device = local
     torch.cuda.set_device(device)
     dev = f"cuda:{device}"
@@ -767,16 +845,16 @@ def serving_arm(args, w: dict, world: int, rank: int, local: int) -> int:
                 "h2d_bytes_per_step": top["h2d_bytes"] // top["queries"],
                 "d2h_bytes_per_step": top["d2h_bytes"] // top["queries"]},
         "gpu_launches": sum(r["launches"] for r in results), "clocks": clocks,
+        "replies_checked": sum(r["queries"] for r in results), "mismatches": mism,
     }
-    print(json.dumps(line), flush=True)
+    pools.clear()
+    expect.clear()
     for d in imported.values():
         d.free()
     for c in ctxs:
         c.close()
-    if mism:
-        log(f"{mism} served replies differ from the replies computed alone")
-        return 1
-    return 0
+    torch.cuda.empty_cache()
+    return line
 
 
 def reference_serving_arm(args, w: dict, world: int, rank: int) -> int:
@@ -811,6 +889,8 @@ def main() -> int:
     ap.add_argument("--workload", default="memory_bound", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", dest="extras", action="store_false",
+                    help="default workload only: leave out the batched and serving sub-objects")
     ap.add_argument("--elements", type=int, default=0,
                     help="override the element count (profiling runs on a smaller case): a d=1 workload's "
                          "grid follows it, a d>1 workload keeps its grid")

@@ -334,6 +334,31 @@ def ref_run(N: int, m: int, n: list[int], alpha: int, db: np.ndarray, nfiles: in
         return out
 
 
+def ref_bench(N: int, m: int, n: list[int], alpha: int, db: np.ndarray, nfiles: int, L: int, keyseed: int,
+              chosen: int, reps: int, warmup: int = 0, threads: int | None = None) -> dict:
+    """The reference answering repeated queries on one imported database (xpir_ref bench):
+    the JSON summary with the per-repetition reply times in 'reply_s'."""
+    with tempfile.TemporaryDirectory() as td:
+        t = Path(td)
+        np.ascontiguousarray(db, dtype=np.uint8).tofile(t / "db.bin")
+        args = {"params": params_str(N, m), "alpha": alpha, "d": len(n), "n": ",".join(map(str, n)),
+                "nfiles": nfiles, "eltbytes": L, "db": t / "db.bin", "keyseed": keyseed, "chosen": chosen,
+                "reps": reps, "warmup": warmup}
+        return _ref("bench", args, threads)
+
+
+def host_cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), for the record of a CPU timing."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def ref_extract(N: int, m: int, n: list[int], alpha: int, L: int, keyseed: int, reply: np.ndarray) -> np.ndarray:
     """Decrypt replies with the reference's PIRReplyExtraction and the seeded key."""
     with tempfile.TemporaryDirectory() as td:

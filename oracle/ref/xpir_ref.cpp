@@ -9,6 +9,7 @@
 //
 // Commands (all binary files are raw little-endian):
 //   run      full PIR round trip; dumps query, imported DB, replies, recovered element
+//   bench    one query, one import, then repeated timed replies (the benchmark's reference arm)
 //   extract  decrypt a given reply (e.g. one produced on the GPU) with the seeded key
 //   key      write the seeded secret key (NTT domain) for the oracle's and GPU's decryption
 //   tables   dump the NTT tables built by NFLlib::configureNTT (crypto/NFLlib.cpp:44-194)
@@ -274,6 +275,60 @@ int cmd_run(const Args &a) {
   return ok == 0 ? 1 : 0;
 }
 
+// Repeated replies against one imported database, the way a server answers successive
+// queries: the reference's query (PIRQueryGenerator) is pushed once, the database is
+// imported once, then generateReply runs --warmup + --reps times on the same generator,
+// each timed with omp_get_wtime at the boundaries the reference prints
+// (PIRReplyGeneratorNFL_internal.cpp:354-444).  The benchmark's reference arm.
+int cmd_bench(const Args &a) {
+  PIRParameters params = pir_params(a);
+  HomomorphicCrypto *crypto = make_crypto(a, params);
+  NFLLWE *lwe = dynamic_cast<NFLLWE *>(crypto);
+  const uint64_t L = a.u64("eltbytes");
+  const uint64_t reps = a.u64("reps", 1), warmup = a.u64("warmup", 0);
+  std::vector<element_t> *elts = load_db(a);
+  DBVectorProcessor db(*elts);
+  double t0 = omp_get_wtime();
+  PIRQueryGenerator q_generator(params, *crypto);
+  q_generator.generateQuery(a.u64("chosen", 0));
+  const double t_query = omp_get_wtime() - t0;
+  PIRReplyGenerator *r_generator = new PIRReplyGenerator(params, *crypto, &db);
+  char *q;
+  t0 = omp_get_wtime();
+  while (q_generator.popQuery(&q)) r_generator->pushQuery(q);
+  const double t_push = omp_get_wtime() - t0;
+  t0 = omp_get_wtime();
+  imported_database *imported_db = r_generator->importData(0, L);
+  const double t_import = omp_get_wtime() - t0;
+  std::vector<double> reply_s;
+  uint64_t nrep = 0;
+  for (uint64_t i = 0; i < warmup + reps; i++) {
+    t0 = omp_get_wtime();
+    r_generator->generateReply(imported_db);
+    const double t = omp_get_wtime() - t0;
+    if (i >= warmup) reply_s.push_back(t);
+    char *rep;
+    nrep = 0;
+    while (r_generator->popReply(&rep)) {
+      free(rep);
+      nrep++;
+    }
+  }
+  print_info(lwe, params);
+  result(", \"polys_per_element\": %llu, \"nb_elements\": %llu, \"n_replies\": %llu, \"query_s\": %.6f, "
+         "\"push_s\": %.6f, \"import_s\": %.6f, \"omp_threads\": %d, \"reply_s\": [",
+         (unsigned long long)imported_db->polysPerElement, (unsigned long long)imported_db->nbElements,
+         (unsigned long long)nrep, t_query, t_push, t_import, omp_get_max_threads());
+  for (size_t i = 0; i < reply_s.size(); i++) result(i ? ", %.6f" : "%.6f", reply_s[i]);
+  result("]}\n");
+  delete imported_db;
+  r_generator->freeQueries();
+  delete r_generator;
+  delete crypto;
+  delete elts;
+  return 0;
+}
+
 // Decrypt given replies with the seeded key (PIRReplyExtraction, libpir.cpp:171-201).
 int cmd_extract(const Args &a) {
   PIRParameters params = pir_params(a);
@@ -418,7 +473,7 @@ int cmd_ntt(const Args &a) {
 
 int main(int argc, char **argv) {
   if (argc < 2) {
-    fprintf(stderr, "usage: xpir_ref run|extract|key|tables|bitsplit|deser|ntt|info [--key value ...]\n");
+    fprintf(stderr, "usage: xpir_ref run|bench|extract|key|tables|bitsplit|deser|ntt|info [--key value ...]\n");
     return 2;
   }
   std::string cmd = argv[1];
@@ -431,6 +486,7 @@ int main(int argc, char **argv) {
   dup2(sink, 1);
   close(sink);
   if (cmd == "run") return cmd_run(a);
+  if (cmd == "bench") return cmd_bench(a);
   if (cmd == "extract") return cmd_extract(a);
   if (cmd == "tables") return cmd_tables(a);
   if (cmd == "bitsplit") return cmd_bitsplit(a, false);

@@ -26,8 +26,10 @@ def test_reference_arm_line_follows_the_contract():
                 "scaling", "vs_baseline", "dtype", "data", "config"):
         assert key in d, key
     assert d["unit"] == "GB/s" and d["higher_is_better"] is True and d["value"] > 0
-    assert d["config"]["workload"].startswith("memory-bound") and d["config"]["elements_sampled"] == 2000
+    assert d["config"]["workload"].startswith("memory-bound") and d["config"]["elements_timed"] == 2000
+    assert d["config"]["same_config"] is True  # every element of the (here reduced) workload is timed
     cb = d["cpu_baseline"]
     assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["value"] == d["value"]
+    assert cb["cpu_model"] and len(d["reply_s"]) == d["steps"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
 
