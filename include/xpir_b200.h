@@ -83,6 +83,16 @@ XPIR_B200_API int xpir_b200_ctx_stream(xpir_b200_ctx *ctx, void **stream);
 XPIR_B200_API int xpir_b200_ctx_synchronize(xpir_b200_ctx *ctx);
 /* Number of engine kernels launched on this context so far. */
 XPIR_B200_API int xpir_b200_ctx_launch_count(xpir_b200_ctx *ctx, uint64_t *count);
+/* Test support for the reply kernel's bounded waits; no counterpart in the reference.
+ * Every wait in the reply kernel gives up after a fixed number of polls (about 2.6 s),
+ * records the failure and lets the kernel return, so that a stalled pipeline ends in
+ * XPIR_B200_ERR_TIMEOUT instead of a hang.  For the following xpir_b200_reply calls on
+ * this context: spin_limit > 0 shortens the limit of the consumers' waits and of the copy
+ * producer's ring (the producer's final wait for its own copies in flight keeps the full
+ * limit), and withhold_tile >= 0 makes every reply CTA's copy producer stop before that
+ * tile's copies, so that the waits for it run out and the call returns
+ * XPIR_B200_ERR_TIMEOUT with nothing left in flight.  (0, -1) restores normal operation. */
+XPIR_B200_API int xpir_b200_ctx_set_wait_test(xpir_b200_ctx *ctx, uint32_t spin_limit, int32_t withhold_tile);
 
 /* ---- database import -------------------------------------------------------------- */
 /* Imports a database for queries whose aggregation is `alpha` and whose first dimension

@@ -80,7 +80,8 @@ def test_noalloc_first_call_allocates_nothing(engine, oracle):
     with engine.Context(N, m) as ctx:
         db = ctx.import_db(random_db(76, F, L), F, L, 1, b)
         q_dev = torch.from_numpy(q.view(np.int64)).cuda()
-        out_dev = torch.full((2 * m * N,), -1, dtype=torch.int64, device="cuda")
+        count_want = engine.reply_count(L, 1, len(n), b, N, m)
+        out_dev = torch.full((count_want * 2 * m * N,), -1, dtype=torch.int64, device="cuda")
         ctx.synchronize()
         torch.cuda.synchronize()
         free_before, _ = torch.cuda.mem_get_info()

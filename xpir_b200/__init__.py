@@ -76,6 +76,7 @@ def _load():
         L.xpir_b200_ctx_stream.argtypes = [vp, ctypes.POINTER(vp)]
         L.xpir_b200_ctx_synchronize.argtypes = [vp]
         L.xpir_b200_ctx_launch_count.argtypes = [vp, ctypes.POINTER(c_u64)]
+        L.xpir_b200_ctx_set_wait_test.argtypes = [vp, c_u32, ctypes.c_int32]
         L.xpir_b200_db_import.argtypes = [vp, vp, c_u64, c_u64, c_u64, c_u32, c_u32, ctypes.c_int,
                                           ctypes.POINTER(vp)]
         L.xpir_b200_db_free.argtypes = [vp]
@@ -332,6 +333,10 @@ class Context:
         _check(_load().xpir_b200_autotune(self.handle, db.handle, len(n), narr, _ptr(query), ctypes.byref(tile)),
                "autotune")
         return tile.value
+
+    def set_wait_test(self, spin_limit: int = 0, withhold_tile: int = -1) -> None:
+        """Test support of the reply kernel's bounded waits (xpir_b200_ctx_set_wait_test)."""
+        _check(_load().xpir_b200_ctx_set_wait_test(self.handle, spin_limit, withhold_tile), "set_wait_test")
 
     def set_level_tile(self, P: int, n_i: int, groups: int, tile: int) -> None:
         """Pins the reply kernel's tile shape for one level shape (-1: default choice)."""

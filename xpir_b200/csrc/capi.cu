@@ -189,6 +189,14 @@ int xpir_b200_ctx_synchronize(xpir_b200_ctx *ctx) {
   return XPIR_B200_OK;
 }
 
+int xpir_b200_ctx_set_wait_test(xpir_b200_ctx *ctx, uint32_t spin_limit, int32_t withhold_tile) {
+  if (!ctx || withhold_tile < -1) return XPIR_B200_ERR_ARG;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  ctx->wait_test.spin_limit = spin_limit;
+  ctx->wait_test.withhold_tile = withhold_tile;
+  return XPIR_B200_OK;
+}
+
 int xpir_b200_ctx_launch_count(xpir_b200_ctx *ctx, uint64_t *count) {
   if (!ctx || !count) return XPIR_B200_ERR_ARG;
   *count = ctx->launches;
@@ -345,6 +353,7 @@ int xpir_b200_reply(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, cons
     uint32_t launched = 0;
     ReplyLevelArgs a{in, in_real, Ps[lvl], groups[lvl], n[lvl], dq, rep};
     a.write_idle = last;
+    a.wait_test = ctx->wait_test;
     const uint64_t active = active_groups(in_real, n[lvl], groups[lvl]);
     const cudaError_t le = launch_reply_level(a, ps, dm, ctx->stream, &launched, ctx->status_dev,
                                               tuned_tile(ctx, Ps[lvl], n[lvl], groups[lvl]));

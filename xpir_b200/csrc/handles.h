@@ -13,6 +13,7 @@
 #include <tuple>
 #include <vector>
 
+#include "kernels.h"
 #include "params.h"
 
 struct xpir_b200_db;
@@ -43,6 +44,7 @@ struct xpir_b200_ctx {
   std::set<xpir_b200_db *> dbs;  // databases imported through this context
   TuneTable tuned;
   uint64_t tune_epoch = 0;  // bumped by every autotune (invalidates captured batches)
+  xpir::WaitTest wait_test;  // test support of the bounded waits (xpir_b200_ctx_set_wait_test)
   std::vector<std::shared_ptr<BatchPlan>> plans;  // captured batches (batch.cu)
 };
 

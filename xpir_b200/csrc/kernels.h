@@ -54,6 +54,16 @@ cudaError_t launch_import(const AggSource &src, uint64_t groups, uint64_t P, con
                           const DevModuli &dm, const uint64_t *tables, uint64_t *out, cudaStream_t stream,
                           const ImportRows *rows = nullptr, uint32_t *launches = nullptr);
 
+// Test support for the reply kernel's bounded waits (xpir_b200_ctx_set_wait_test): a
+// shorter limit for the waits of the consumer warps and of the copy producer's ring, and
+// a tile whose copies the producer never issues (-1: none), so that the waits for that
+// tile run out, the kernel records kStatusWaitTimeout and returns.  The producer's final
+// wait for its own copies in flight keeps the full limit.
+struct WaitTest {
+  uint32_t spin_limit = 0;  // 0: the default limit (sm100.cuh kSpinLimit)
+  int32_t withhold_tile = -1;
+};
+
 // One recursion level of the reply (pir/replyGenerator/PIRReplyGeneratorNFL_internal.cpp:511-595):
 // for group g < n_groups and poly cp < P, the in-order lazy Shoup accumulation over the
 // n_i slots of the group; slot q reads DB element g*n_i + q, an all-zero element when
@@ -70,6 +80,7 @@ struct ReplyLevelArgs {
   // A level whose replies only feed the next level's import (which knows they are zero,
   // see ImportRows) skips it.
   bool write_idle = true;
+  WaitTest wait_test;
 };
 // `status` is a device-visible int that a kernel sets to a nonzero KernelStatus when one
 // of its bounded waits gives up (sm100.cuh); the caller clears and reads it.

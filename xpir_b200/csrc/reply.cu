@@ -87,6 +87,7 @@ struct LevelShape {
   uint64_t n_real, P, n_i;
   uint32_t N, m, col_blocks;
   uint64_t groups;  // groups with data (GRP tiles write only these)
+  WaitTest wait_test;
 };
 
 
@@ -118,6 +119,7 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
   const uint32_t delta = (uint32_t)dm.shoup_delta[c];
   const uint64_t np = opaque(0 - p);
   const uint32_t tiles = (uint32_t)((sh.n_i + E - 1) / E);
+  const uint32_t lim = sh.wait_test.spin_limit ? sh.wait_test.spin_limit : kSpinLimit;
 
   if (threadIdx.x == 0) {
     // Every consumer thread arrives on the release barriers, so each thread's own
@@ -144,7 +146,8 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
       uint32_t t = 0;
       for (; t < tiles; ++t) {
         const int s = (int)(t % NS);
-        if (t >= (uint32_t)NS && !mbar_wait(empty + s, (t / NS - 1) & 1)) {
+        if ((int32_t)t == sh.wait_test.withhold_tile) break;  // test support: starve the consumers
+        if (t >= (uint32_t)NS && !mbar_wait(empty + s, (t / NS - 1) & 1, lim)) {
           ok = false;
           break;
         }
@@ -169,8 +172,8 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
     const int ct = threadIdx.x - 32;
     for (uint32_t t = 0; t < tiles && ok; ++t) {
       const int s = (int)(t % NS), b = (int)(t % TB);
-      if (!mbar_wait(full + s, (t / NS) & 1)) ok = false;
-      if (ok && t >= (uint32_t)TB && !mbar_wait(tempty + b, (t / TB - 1) & 1)) ok = false;
+      if (!mbar_wait(full + s, (t / NS) & 1, lim)) ok = false;
+      if (ok && t >= (uint32_t)TB && !mbar_wait(tempty + b, (t / TB - 1) & 1, lim)) ok = false;
       if (!ok) break;
       const uint64_t *xst = xs + s * S::kX + off;
       const uint64_t *qst = qs + s * S::kQ + off;
@@ -234,7 +237,7 @@ __device__ __forceinline__ void reply_tile(const CUtensorMap *tm_db, const CUten
     uint64_t rop = 0;
     for (uint32_t t = 0; t < tiles; ++t) {
       const int b = (int)(t % TB);
-      if (!mbar_wait(tfull + b, (t / TB) & 1)) {
+      if (!mbar_wait(tfull + b, (t / TB) & 1, lim)) {
         ok = false;
         break;
       }
@@ -350,7 +353,7 @@ cudaError_t launch_c(const ReplyLevelArgs &a, const ParamSet &ps, const DevModul
   if (GRP && (a.P != 1 || ((groups + C - 1) / C * C + 1) * a.n_i >= (1ull << 31))) return cudaErrorInvalidValue;
   const uint32_t col_blocks = GRP ? 1 : (uint32_t)((a.P + C - 1) / C);
   const uint64_t blocks = GRP ? (groups + C - 1) / C : groups;
-  LevelShape sh{a.n_real, a.P, a.n_i, ps.N, ps.m, col_blocks, groups};
+  LevelShape sh{a.n_real, a.P, a.n_i, ps.N, ps.m, col_blocks, groups, a.wait_test};
   if (blocks > 0x7fffffffull || (uint64_t)ps.m * col_blocks > 65535) return cudaErrorInvalidValue;
   dim3 grid((unsigned)blocks, (ps.N + W - 1) / W, (unsigned)(ps.m * col_blocks));
   kern<<<grid, S::kThreads, S::kBytes, stream>>>(tm_db, tm_q, a.out, sh, dm, status);
