@@ -891,6 +891,8 @@ def main() -> int:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", dest="extras", action="store_false",
                     help="default workload only: leave out the batched and serving sub-objects")
+    ap.add_argument("--batch-div", type=int, default=1,
+                    help="batched workload: divide the query count of every class (profiling runs)")
     ap.add_argument("--elements", type=int, default=0,
                     help="override the element count (profiling runs on a smaller case): a d=1 workload's "
                          "grid follows it, a d>1 workload keeps its grid")
@@ -902,6 +904,17 @@ def main() -> int:
             return reference_serving_arm(args, w, world, rank)
         return serving_arm(args, w, world, rank, local)
     if args.workload == "batched":
+        if args.elements or args.batch_div > 1:
+            # A smaller batch of the same three classes (profiling): E elements, class
+            # counts divided by batch_div, the d = 2 grid [E / 256, 256].
+            E = args.elements or w["F"]
+            if E % 1024:
+                ap.error("--elements: the batched workload needs a multiple of 1024")
+            w.update(F=E, classes=[(max(1, c // args.batch_div), n, a) for c, n, a in
+                                   [(w["classes"][0][0], [E], 1), (w["classes"][1][0], [E // 4], 4),
+                                    (w["classes"][2][0], [E // 256, 256], 1)]],
+                     desc=f"batched (reduced): LWE:80:2048:120, {E} x 8 KB, classes d1/a1, d1/a4, d2 "
+                          f"[{E // 256}, 256], counts divided by {args.batch_div}")
         if args.impl == "reference":
             return reference_batched_arm(args, w, world, rank)
         return batched_arm(args, w, world, rank, local)

@@ -90,7 +90,7 @@ def test_graph_of_a_freed_database_is_not_replayed(engine):
     torch = pytest.importorskip("torch")
     N, m, n = 2048, 2, [400]
     b = engine.bits_per_coeff(N, m, n[0])
-    assert engine.polys_per_element(3000, 1, b, N) == 1 and engine.polys_per_element(6000, 1, b, N) == 2
+    assert engine.polys_per_element(3000, 1, b, N) == 1 and engine.polys_per_element(12000, 1, b, N) == 2
     with engine.Context(N, m) as ctx:
         q = random_query(41, n, N, m, engine.moduli(m))
         qd = to_dev(torch, q)
@@ -100,7 +100,7 @@ def test_graph_of_a_freed_database_is_not_replayed(engine):
         assert ctx.reply_batch([(db1, n, qd, out)], use_graph=True) == [1]  # captured
         assert np.array_equal(out[: want1.size].cpu().numpy().view(np.uint64), want1)
         db1.free()
-        db2 = ctx.import_db(random_db(43, 200, 6000), 200, 6000, 1, b)
+        db2 = ctx.import_db(random_db(43, 200, 12000), 200, 12000, 1, b)
         want2 = ctx.reply(db2, n, q)
         out.fill_(-1)
         assert ctx.reply_batch([(db2, n, qd, out)], use_graph=True) == [2]
