@@ -70,9 +70,10 @@ def build_pir(force: bool = False) -> Path:
 def build_xpir(xpir_ref: str) -> Path:
     """XPIR's pir library with the B200 engine plugged in (xpir_b200/xpir/Makefile):
     XPIR's sources from `xpir_ref` with libpir.cpp and PIRReplyGeneratorFactory.cpp
-    replaced by the B200 ones, archived as xpir_b200/xpir/_build/libpir_b200.a."""
-    res = subprocess.run(["make", "-s", "-j8", "-C", str(PKG / "xpir"), f"XPIR_REF={xpir_ref}"], capture_output=True,
-                         text=True)
+    replaced by the B200 ones, archived as xpir_b200/xpir/_build/libpir_b200.a, and XPIR's
+    own server and client linked with it (xpir_b200/xpir/_build/pir_server, pir_client)."""
+    res = subprocess.run(["make", "-s", "-j8", "-C", str(PKG / "xpir"), "all", "apps", f"XPIR_REF={xpir_ref}"],
+                         capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"building the XPIR binding failed:\n{res.stdout}\n{res.stderr}")
     return PKG / "xpir" / "_build" / "libpir_b200.a"

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <string>
 #include <cassert>
+#include <iomanip>
 #endif
 #include <semaphore.h>  // SEM_VALUE_MAX, used by pir/shared_queue.hpp
 #endif
