@@ -43,8 +43,8 @@ METRIC = "reply-gen DB GB/s vs HBM peak; batched vs plain queries/s; p50/p99 lat
 # reply) of one reply_tma_kernel launch on the memory-bound workload, from one
 # `ncu --set full` capture of a 10,000-element case of the same kernel and grid
 # (traffic grows with the elements: each is one DB row and one query ciphertext):
-# (999.2 + 3.5) MB / 983.1 MB.
-REPLY_TRAFFIC_PER_ALGORITHMIC_BYTE = 1.0199
+# (995.5 + 3.7) MB / 983.1 MB.
+REPLY_TRAFFIC_PER_ALGORITHMIC_BYTE = 1.0164
 
 WORKLOADS = {
     # name: N, m, n levels, alpha, elements, element bytes, chosen index, cpu-sample elements
