@@ -1,7 +1,8 @@
 """GPU tests of the serving loop (xpir_b200_server_*): queries from several clients on
 databases of two parameter sets, admitted by a device-memory budget and batched as they
 arrive.  Every served reply must be bit-identical to the single-query reply of the same
-query computed alone (integer work, no tolerance)."""
+query computed alone, and that reply to the oracle restatement's (integer work, no
+tolerance)."""
 from __future__ import annotations
 
 import threading
@@ -14,19 +15,27 @@ from helpers import random_db, random_query
 pytestmark = pytest.mark.gpu
 
 
-def make_load(engine, ctxs):
+def make_load(engine, ctxs, oracle=None):
     """Databases on two parameter sets with d in {1, 2} and alpha in {1, 4}, and a list of
-    (db, n, host query, expected reply) of 4 queries per database."""
+    (db, n, host query, expected reply) of 4 queries per database.  With the oracle, each
+    expected reply is first checked against the restatement's."""
     (ctx_a, (Na, ma)), (ctx_b, (Nb, mb)) = ctxs
     specs = [(ctx_a, Na, ma, 900, 2000, [900], 1), (ctx_a, Na, ma, 900, 2000, [30, 30], 1),
              (ctx_b, Nb, mb, 1200, 700, [300], 4), (ctx_b, Nb, mb, 1200, 700, [20, 15], 4)]
     load, dbs = [], []
     for k, (ctx, N, m, F, L, n, alpha) in enumerate(specs):
-        db = ctx.import_db(random_db(300 + k, F, L), F, L, alpha, engine.bits_per_coeff(N, m, n[0]))
+        elems = random_db(300 + k, F, L)
+        b = engine.bits_per_coeff(N, m, n[0])
+        db = ctx.import_db(elems, F, L, alpha, b)
         dbs.append(db)
+        imported = oracle.import_db(elems, F, L, alpha, b, N, m) if oracle else None
         for j in range(4):
             q = random_query(7000 + 10 * k + j, n, N, m, engine.moduli(m))
-            load.append((db, n, q, ctx.reply(db, n, q)))
+            want = ctx.reply(db, n, q)
+            if oracle:
+                P = oracle.polys_for_bits(8 * alpha * L, b, N)
+                assert np.array_equal(want, oracle.reply(imported, -(-F // alpha), P, n, q, b, N, m))
+            load.append((db, n, q, want))
     return load, dbs
 
 
@@ -53,9 +62,9 @@ def serve_all(engine, server, load, clients=4):
     return outs, counts
 
 
-def test_served_replies_equal_replies_alone(engine):
+def test_served_replies_equal_replies_alone(engine, oracle):
     with engine.Context(1024, 1) as ca, engine.Context(2048, 2) as cb:
-        load, _ = make_load(engine, [(ca, (1024, 1)), (cb, (2048, 2))])
+        load, _ = make_load(engine, [(ca, (1024, 1)), (cb, (2048, 2))], oracle)
         with engine.Server([ca, cb], device_budget_bytes=1 << 30, max_batch=16) as srv:
             outs, counts = serve_all(engine, srv, load)
             st = srv.stats()
