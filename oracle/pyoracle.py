@@ -35,7 +35,7 @@ def build(reference_root: str | None = None) -> None:
     subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so"], check=True, env=env)
     ref = reference_root or os.environ.get("XPIR_REF", "")
     if ref and Path(ref, "crypto", "NFLlib.cpp").exists():
-        subprocess.run(["make", "-s", "-j8", "-C", str(HERE), "ref", "simplepir", f"XPIR_REF={ref}"], check=True,
+        subprocess.run(["make", "-s", "-j8", "-C", str(HERE), "ref", "simplepir", "apps", f"XPIR_REF={ref}"], check=True,
                        env=env)
 
 

@@ -10,6 +10,10 @@ in server-driven mode (-z: the first client configures it and the imported datab
 in HBM for the next clients), the client with forced crypto parameters, recursion level and
 aggregation (-r ... --reclvl d --alpha a -c), run twice, and the retrieved file compared with
 the database's first element (the directory's first entry, as DBDirectoryProcessor lists it).
+
+The same loopback also runs without a GPU against XPIR's server built with the stock libpir
+and factory (oracle/_ref/pir_server, the CPU reply generator): it checks the Boost
+stand-ins of xpir_b200/xpir/compat and this harness on every CPU run.
 """
 from __future__ import annotations
 
@@ -24,9 +28,8 @@ import pytest
 ROOT = Path(__file__).resolve().parent.parent
 BUILD = ROOT / "xpir_b200" / "xpir" / "_build"
 SERVER, CLIENT = BUILD / "pir_server", BUILD / "pir_client"
+STOCK_SERVER = ROOT / "oracle" / "_ref" / "pir_server"
 PORT = 1234  # XPIR's server listens on its default port (its -p value is never applied)
-
-pytestmark = pytest.mark.gpu
 
 
 def listening(port: int) -> bool:
@@ -44,10 +47,8 @@ def listening(port: int) -> bool:
     return False
 
 
-@pytest.mark.parametrize("reclvl,alpha,params", [(1, 1, "LWE:.*:4096:120"), (2, 1, "LWE:.*:4096:120"),
-                                                 (1, 2, "LWE:.*:2048:60"), (3, 1, "LWE:.*:4096:180")])
-def test_xpir_server_and_client_over_loopback(tmp_path, reclvl, alpha, params):
-    for exe in (SERVER, CLIENT):
+def loopback(server_exe: Path, tmp_path: Path, reclvl: int, alpha: int, params: str) -> None:
+    for exe in (server_exe, CLIENT):
         if not exe.exists():
             pytest.skip(f"{exe.relative_to(ROOT)} is not built (built by __graft_entry__.build() from the XPIR sources)")
     for _ in range(60):  # a previous server's port must be free
@@ -64,7 +65,7 @@ def test_xpir_server_and_client_over_loopback(tmp_path, reclvl, alpha, params):
     first = os.listdir(tmp_path / "db")[0]
     want = (tmp_path / "db" / first).read_bytes()
 
-    server = subprocess.Popen([str(SERVER), "-z"], cwd=tmp_path, stdout=open(tmp_path / "server.out", "w"),
+    server = subprocess.Popen([str(server_exe), "-z"], cwd=tmp_path, stdout=open(tmp_path / "server.out", "w"),
                               stderr=subprocess.STDOUT)
     try:
         for _ in range(300):
@@ -89,3 +90,14 @@ def test_xpir_server_and_client_over_loopback(tmp_path, reclvl, alpha, params):
         except subprocess.TimeoutExpired:
             server.kill()
             server.wait(timeout=30)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("reclvl,alpha,params", [(1, 1, "LWE:.*:4096:120"), (2, 1, "LWE:.*:4096:120"),
+                                                 (1, 2, "LWE:.*:2048:60"), (3, 1, "LWE:.*:4096:180")])
+def test_xpir_server_on_gpu_and_client_over_loopback(tmp_path, reclvl, alpha, params):
+    loopback(SERVER, tmp_path, reclvl, alpha, params)
+
+
+def test_stock_xpir_server_and_client_over_loopback(tmp_path):
+    loopback(STOCK_SERVER, tmp_path, 2, 1, "LWE:.*:4096:120")
