@@ -59,6 +59,10 @@ WORKLOADS = {
     "batched": dict(N=2048, m=2, F=65536, L=8192, sample=8192,
                     classes=[(32, [65536], 1), (16, [16384], 4), (16, [256, 256], 1)],
                     desc="batched: LWE:80:2048:120, 65536 x 8 KB, 64 queries (32 d1/a1, 16 d1/a4, 16 d2 256x256)"),
+    # Client-side query generation on the GPU: the memory-bound workload's query (100,000
+    # ciphertexts, 6.55 GB) for element 54,321, PIRQueryGenerator with the reference's PRNG.
+    "querygen": dict(N=2048, m=2, n=[100000], chosen=54321, sample=100000,
+                     desc="query generation: LWE:80:2048:120, d=1, 100000 ciphertexts (6.55 GB) for element 54321"),
     # Serving loop over three resident databases, one lane (context) each.  mix: (database,
     # d, alpha, weight) of the admitted shapes; grids from the client optimizer's rule.
     "serving": dict(dbs=[("DB1", 1024, 1, 200000, 2048), ("DB2", 2048, 2, 100000, 8192),
@@ -563,6 +567,72 @@ def measure_batched(args, w: dict, world: int, rank: int, local: int, dist) -> d
     return line
 
 
+def querygen_arm(args, w: dict, world: int, rank: int, local: int) -> int:
+    """Client-side query generation (xpir_b200_generate_query) into HBM, one query of
+    sum(n) ciphertexts per step; value = ciphertexts/s.  Replicas on N GPUs."""
+    import torch
+
+    import xpir_b200
+    from oracle import pyoracle as po
+
+    dist = init_dist(world, local)
+    torch.cuda.set_device(local)
+    N, m, n = w["N"], w["m"], w["n"]
+    b = xpir_b200.bits_per_coeff(N, m, n[0])
+    ctx = xpir_b200.Context(N, m, device=local)
+    key = po.seeded_prng_key(7 + rank)
+    sk = ctx.generate_secret_key(key, 0)
+    out = torch.empty(sum(n) * 2 * m * N, dtype=torch.int64, device=f"cuda:{local}")
+    stream = torch.cuda.ExternalStream(ctx.stream, device=local)
+    for _ in range(args.warmup):
+        ctx.generate_query(key, 1, sk, n, w["chosen"], b, out=out)
+    torch.cuda.synchronize()
+    launches0 = ctx.launch_count
+    if dist is not None:
+        dist.barrier()
+    with ClockSampler(local) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            ctx.generate_query(key, 1, sk, n, w["chosen"], b, out=out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    (ms,) = max_over_ranks(dist, [ms], f"cuda:{local}")
+    count = sum(n)
+    if rank == 0:
+        peaks = measured_peaks()
+        out_bytes = count * 2 * m * N * 8
+        achieved = out_bytes / (ms / 1e3) / 1e9
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline and po.ref_available():
+            r = po.ref_querygen(N, m, n, w["chosen"], keyseed=7, threads=os.cpu_count() or 1)
+            cpu = {"value": round(count / r["query_s"], 2), "unit": "ciphertexts/s", "cores": r["omp_threads"],
+                   "kind": "reference", "cpu_model": po.host_cpu_model(),
+                   "sample": f"the full query ({count} ciphertexts) by the reference's PIRQueryGenerator, "
+                             f"{r['query_s']:.2f} s"}
+        line = {
+            "metric": METRIC, "value": round(world * count / (ms / 1e3), 1), "unit": "ciphertexts/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic: seeded PRNG key; the secret key and noise from the reference's Salsa20 stream",
+            "config": {"workload": w["desc"], "N": N, "moduli": m, "n": n, "bits_per_coeff": b,
+                       "l2": "output larger than L2 (no flush needed)",
+                       "parallelism": f"replicas{world}" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": None,
+                         "kernel": "encrypt_kernel (query written once)", "peak_source": peaks["source"],
+                         "algorithmic_bytes_per_launch": out_bytes, "kernel_ms": round(ms, 4)},
+            "cpu_baseline": cpu, "e2e": None,
+            "gpu_launches": ctx.launch_count - launches0, "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
 def reference_batch_rate(w: dict, threads: int) -> dict:
     """The reference answering the batch's queries one at a time on the full database: one
     query of each class timed (xpir_ref bench, one repetition); the batch takes the sum of
@@ -903,6 +973,32 @@ def main() -> int:
         if args.impl == "reference":
             return reference_serving_arm(args, w, world, rank)
         return serving_arm(args, w, world, rank, local)
+    if args.workload == "querygen":
+        if args.elements:
+            w.update(n=[args.elements], chosen=min(w["chosen"], args.elements - 1),
+                     desc=w["desc"].replace("100000 ciphertexts (6.55 GB)", f"{args.elements} ciphertexts"))
+        if args.impl == "reference":
+            if rank != 0:
+                return 0
+            from oracle import pyoracle as po
+
+            if not po.ref_available():
+                print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/xpir_ref is not built "
+                                  "(query generation has no port in the oracle)"}))
+                return 0
+            r = po.ref_querygen(w["N"], w["m"], w["n"], w["chosen"], keyseed=7, threads=os.cpu_count() or 1)
+            v = round(sum(w["n"]) / r["query_s"], 2)
+            print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "ciphertexts/s",
+                              "n_gpus": args.gpus, "steps": 1, "warmup": 0, "ms_per_step": round(r["query_s"] * 1e3, 3),
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+                              "data": "seeded key; the reference's PIRQueryGenerator", "config": {"workload": w["desc"]},
+                              "cpu_baseline": {"value": v, "unit": "ciphertexts/s", "cores": r["omp_threads"],
+                                               "kind": "reference", "cpu_model": po.host_cpu_model(),
+                                               "sample": "the full query"},
+                              "e2e": {"value": v, "unit": "ciphertexts/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}))
+            return 0
+        return querygen_arm(args, w, world, rank, local)
     if args.workload == "batched":
         if args.elements or args.batch_div > 1:
             # A smaller batch of the same three classes (profiling): E elements, class

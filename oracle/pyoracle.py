@@ -347,6 +347,13 @@ def ref_bench(N: int, m: int, n: list[int], alpha: int, db: np.ndarray, nfiles: 
         return _ref("bench", args, threads)
 
 
+def ref_querygen(N: int, m: int, n: list[int], chosen: int, keyseed: int, threads: int | None = None) -> dict:
+    """The reference's client-side query generation alone (xpir_ref querygen)."""
+    args = {"params": params_str(N, m), "alpha": 1, "d": len(n), "n": ",".join(map(str, n)), "keyseed": keyseed,
+            "chosen": chosen}
+    return _ref("querygen", args, threads)
+
+
 def host_cpu_model() -> str:
     """The host CPU's model name (/proc/cpuinfo), for the record of a CPU timing."""
     try:

@@ -10,6 +10,7 @@
 // Commands (all binary files are raw little-endian):
 //   run      full PIR round trip; dumps query, imported DB, replies, recovered element
 //   bench    one query, one import, then repeated timed replies (the benchmark's reference arm)
+//   querygen the client's query generation alone, timed
 //   extract  decrypt a given reply (e.g. one produced on the GPU) with the seeded key
 //   key      write the seeded secret key (NTT domain) for the oracle's and GPU's decryption
 //   tables   dump the NTT tables built by NFLlib::configureNTT (crypto/NFLlib.cpp:44-194)
@@ -329,6 +330,28 @@ int cmd_bench(const Args &a) {
   return 0;
 }
 
+// Client-side query generation alone (PIRQueryGenerator::generateQuery, pir/libpir.cpp:45-60),
+// timed with omp_get_wtime: the reference side of the benchmark's query-generation workload.
+int cmd_querygen(const Args &a) {
+  PIRParameters params = pir_params(a);
+  HomomorphicCrypto *crypto = make_crypto(a, params);
+  double t0 = omp_get_wtime();
+  PIRQueryGenerator q_generator(params, *crypto);
+  q_generator.generateQuery(a.u64("chosen", 0));
+  const double t_query = omp_get_wtime() - t0;
+  uint64_t count = 0;
+  char *q;
+  while (q_generator.popQuery(&q)) {
+    free(q);
+    count++;
+  }
+  print_info(dynamic_cast<NFLLWE *>(crypto), params);
+  result(", \"ciphertexts\": %llu, \"query_s\": %.6f, \"omp_threads\": %d}\n", (unsigned long long)count, t_query,
+         omp_get_max_threads());
+  delete crypto;
+  return 0;
+}
+
 // Decrypt given replies with the seeded key (PIRReplyExtraction, libpir.cpp:171-201).
 int cmd_extract(const Args &a) {
   PIRParameters params = pir_params(a);
@@ -473,7 +496,7 @@ int cmd_ntt(const Args &a) {
 
 int main(int argc, char **argv) {
   if (argc < 2) {
-    fprintf(stderr, "usage: xpir_ref run|bench|extract|key|tables|bitsplit|deser|ntt|info [--key value ...]\n");
+    fprintf(stderr, "usage: xpir_ref run|bench|querygen|extract|key|tables|bitsplit|deser|ntt|info [--key value ...]\n");
     return 2;
   }
   std::string cmd = argv[1];
@@ -487,6 +510,7 @@ int main(int argc, char **argv) {
   close(sink);
   if (cmd == "run") return cmd_run(a);
   if (cmd == "bench") return cmd_bench(a);
+  if (cmd == "querygen") return cmd_querygen(a);
   if (cmd == "extract") return cmd_extract(a);
   if (cmd == "tables") return cmd_tables(a);
   if (cmd == "bitsplit") return cmd_bitsplit(a, false);

@@ -33,3 +33,14 @@ def test_reference_arm_line_follows_the_contract():
     assert cb["cpu_model"] and len(d["reply_s"]) == d["steps"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
 
+
+def test_query_generation_reference_arm():
+    from oracle import pyoracle as po
+
+    d = run_reference_arm("--workload", "querygen", "--elements", "3000")
+    if not po.ref_available():
+        assert "unavailable" in d
+        return
+    assert d["impl"] == "reference" and d["unit"] == "ciphertexts/s" and d["value"] > 0
+    assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["value"] == d["value"]
+    assert "3000 ciphertexts" in d["config"]["workload"]
