@@ -293,6 +293,10 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
         ctx.reply(dbh, n, q_dev, out_dev)
     torch.cuda.synchronize()
     launches0 = ctx.launch_count
+    # The reply kernels' own CUDA-event times, recorded by the engine around each launch on
+    # its stream (the roofline's kernel time; the step also holds the synchronous call's
+    # host path).
+    ctx.set_kernel_timing(True)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     barrier()
     torch.cuda.synchronize()
@@ -311,6 +315,8 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
         torch.cuda.synchronize()
     barrier()
     launches = ctx.launch_count - launches0
+    kt = ctx.kernel_time()
+    ctx.set_kernel_timing(False)
     step_ms = [a.elapsed_time(b_) for a, b_ in evs]
     # With flushes in the loop the timed work is the sum of the steps' own intervals.
     elapsed_ms = sum(step_ms) if l2_flush else t_start.elapsed_time(t_end)
@@ -342,10 +348,15 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
         peaks = measured_peaks()
         query_bytes = nq * ct_words * 8
         reply_bytes = Pl * ct_words * 8
-        algo_bytes = db_bytes + query_bytes + reply_bytes if len(n) == 1 else None
-        kern_ms = statistics.mean(step_ms)
+        # The dominant kernel is the first level's reply: it reads the whole imported
+        # database and the first dimension's query once and writes one reply per group
+        # that holds data (groups past the last element are not launched).
+        aggregated = math.ceil(F / alpha)
+        active0 = min(math.prod(n[1:]), math.ceil(aggregated / n[0]))
+        algo_bytes = db_bytes + n[0] * ct_words * 8 + active0 * P * ct_words * 8
+        kern_ms = kt["reply_ms"][0] / max(1, kt["reply_launches"][0])
         roofline = None
-        if algo_bytes:
+        if kt["reply_launches"][0]:
             achieved = algo_bytes / (kern_ms / 1e3) / 1e9
             # DRAM traffic cannot be read without a profiler: it is the ncu capture's
             # measured bytes per algorithmic byte of this kernel on this workload, applied
@@ -354,8 +365,13 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
                        if args.workload == "memory_bound" else None)
             roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                         "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
-                        "kernel": "reply_tma_kernel", "peak_source": peaks["source"],
-                        "algorithmic_bytes_per_launch": algo_bytes, "kernel_ms": round(kern_ms, 4)}
+                        "kernel": "reply_tma_kernel" + (" (level 1)" if len(n) > 1 else ""),
+                        "peak_source": peaks["source"], "algorithmic_bytes_per_launch": algo_bytes,
+                        "kernel_ms": round(kern_ms, 4), "kernel_launches_timed": kt["reply_launches"][0]}
+            if len(n) > 1:
+                roofline["later_levels_ms"] = [round(t / max(1, c), 4) for t, c in
+                                               zip(kt["reply_ms"][1:len(n)], kt["reply_launches"][1:len(n)])]
+                roofline["reimport_ms"] = round(kt["import_ms"] / max(1, kt["import_launches"]), 4)
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             r = run_reference(w, steps=1, warmup=0, threads=os.cpu_count() or 1)

@@ -93,6 +93,17 @@ XPIR_B200_API int xpir_b200_ctx_launch_count(xpir_b200_ctx *ctx, uint64_t *count
  * tile's copies, so that the waits for it run out and the call returns
  * XPIR_B200_ERR_TIMEOUT with nothing left in flight.  (0, -1) restores normal operation. */
 XPIR_B200_API int xpir_b200_ctx_set_wait_test(xpir_b200_ctx *ctx, uint32_t spin_limit, int32_t withhold_tile);
+/* Measurement support; no counterpart in the reference.  on != 0: the following
+ * xpir_b200_reply calls on this context record a CUDA event pair on the context's stream
+ * around each level's reply launch and each re-import between levels, and add the
+ * elapsed times up after the call's synchronisation; the sums restart at zero.  on == 0
+ * stops recording (the sums are kept).  Other entry points are not timed. */
+XPIR_B200_API int xpir_b200_ctx_set_kernel_timing(xpir_b200_ctx *ctx, int on);
+/* The sums of xpir_b200_ctx_set_kernel_timing: reply_ms[l] / reply_launches[l] for
+ * recursion level l (XPIR_B200_MAX_LEVELS entries each, level 0 first), and the
+ * re-imports' import_ms / import_launches.  Any pointer may be NULL. */
+XPIR_B200_API int xpir_b200_ctx_kernel_time(xpir_b200_ctx *ctx, double *reply_ms, uint64_t *reply_launches,
+                                            double *import_ms, uint64_t *import_launches);
 
 /* ---- database import -------------------------------------------------------------- */
 /* Imports a database for queries whose aggregation is `alpha` and whose first dimension
@@ -190,6 +201,11 @@ XPIR_B200_API int xpir_b200_extract(xpir_b200_ctx *ctx, const uint64_t *secret_k
                                     uint64_t aggregated_bytes, const void *replies, uint64_t nb_replies,
                                     int replies_on_device, void *plaintext, uint64_t capacity_bytes,
                                     int out_on_device);
+
+/* The client-side entry points (extraction and query generation) take their device
+ * buffers (the key, host-side inputs or outputs staged on the device, the levels'
+ * intermediates) from a stream-ordered pool of the context that keeps freed memory for
+ * the next call; xpir_b200_ctx_destroy releases it. */
 
 /* ---- query generation (client side) ------------------------------------------------ */
 /* The sum(n) query ciphertexts of PIRQueryGenerator::generateQuery for chosen_element

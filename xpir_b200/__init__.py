@@ -77,6 +77,9 @@ def _load():
         L.xpir_b200_ctx_synchronize.argtypes = [vp]
         L.xpir_b200_ctx_launch_count.argtypes = [vp, ctypes.POINTER(c_u64)]
         L.xpir_b200_ctx_set_wait_test.argtypes = [vp, c_u32, ctypes.c_int32]
+        L.xpir_b200_ctx_set_kernel_timing.argtypes = [vp, ctypes.c_int]
+        L.xpir_b200_ctx_kernel_time.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(c_u64),
+                                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(c_u64)]
         L.xpir_b200_db_import.argtypes = [vp, vp, c_u64, c_u64, c_u64, c_u32, c_u32, ctypes.c_int,
                                           ctypes.POINTER(vp)]
         L.xpir_b200_db_free.argtypes = [vp]
@@ -337,6 +340,22 @@ class Context:
     def set_wait_test(self, spin_limit: int = 0, withhold_tile: int = -1) -> None:
         """Test support of the reply kernel's bounded waits (xpir_b200_ctx_set_wait_test)."""
         _check(_load().xpir_b200_ctx_set_wait_test(self.handle, spin_limit, withhold_tile), "set_wait_test")
+
+    def set_kernel_timing(self, on: bool = True) -> None:
+        """Event-timed reply and re-import launches of the following replies
+        (xpir_b200_ctx_set_kernel_timing); switching on restarts the sums."""
+        _check(_load().xpir_b200_ctx_set_kernel_timing(self.handle, int(on)), "set_kernel_timing")
+
+    def kernel_time(self) -> dict:
+        """The sums since set_kernel_timing(True): per recursion level the reply launches'
+        milliseconds and count, and the re-imports' milliseconds and count."""
+        ms = (ctypes.c_double * MAX_LEVELS)()
+        cnt = (ctypes.c_uint64 * MAX_LEVELS)()
+        ims, icnt = ctypes.c_double(), ctypes.c_uint64()
+        _check(_load().xpir_b200_ctx_kernel_time(self.handle, ms, cnt, ctypes.byref(ims), ctypes.byref(icnt)),
+               "kernel_time")
+        return {"reply_ms": list(ms), "reply_launches": [int(c) for c in cnt], "import_ms": ims.value,
+                "import_launches": int(icnt.value)}
 
     def set_level_tile(self, P: int, n_i: int, groups: int, tile: int) -> None:
         """Pins the reply kernel's tile shape for one level shape (-1: default choice)."""

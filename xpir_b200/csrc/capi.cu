@@ -137,6 +137,17 @@ int xpir_b200_ctx_create(xpir_b200_ctx **out, int device, uint32_t N, uint32_t m
   if (rc == XPIR_B200_OK) rc = cuda_status(preload_reply_kernels());
   if (rc == XPIR_B200_OK) rc = cuda_status(prepare_noalloc_scratch(device));
   if (rc == XPIR_B200_OK) rc = cuda_status(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  if (rc == XPIR_B200_OK) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    rc = cuda_status(cudaMemPoolCreate(&ctx->pool, &props));
+  }
+  if (rc == XPIR_B200_OK) {
+    uint64_t keep = UINT64_MAX;
+    rc = cuda_status(cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
   if (rc == XPIR_B200_OK) rc = cuda_status(cudaMalloc(&ctx->d_tables, tables.size() * sizeof(uint64_t)));
   if (rc == XPIR_B200_OK)
     rc = cuda_status(cudaMemcpy(ctx->d_tables, tables.data(), tables.size() * sizeof(uint64_t),
@@ -171,7 +182,11 @@ int xpir_b200_ctx_destroy(xpir_b200_ctx *ctx) {
   if (ctx->tasks_host) cudaFreeHost(ctx->tasks_host);
   ctx->plans.clear();
   if (ctx->status_host) cudaFreeHost(ctx->status_host);
+  for (auto &pair : ctx->timing_ev)
+    for (cudaEvent_t ev : pair)
+      if (ev) cudaEventDestroy(ev);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
   delete ctx;
   return XPIR_B200_OK;
 }
@@ -194,6 +209,38 @@ int xpir_b200_ctx_set_wait_test(xpir_b200_ctx *ctx, uint32_t spin_limit, int32_t
   std::lock_guard<std::mutex> lock(ctx->mu);
   ctx->wait_test.spin_limit = spin_limit;
   ctx->wait_test.withhold_tile = withhold_tile;
+  return XPIR_B200_OK;
+}
+
+int xpir_b200_ctx_set_kernel_timing(xpir_b200_ctx *ctx, int on) {
+  if (!ctx) return XPIR_B200_ERR_ARG;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  if (on) {
+    XPIR_TRY(cudaSetDevice(ctx->device));
+    for (auto &pair : ctx->timing_ev)
+      for (cudaEvent_t &ev : pair)
+        if (!ev) XPIR_TRY(cudaEventCreate(&ev));
+    for (uint32_t l = 0; l < XPIR_B200_MAX_LEVELS; l++) {
+      ctx->reply_ms[l] = 0;
+      ctx->reply_timed[l] = 0;
+    }
+    ctx->import_ms = 0;
+    ctx->import_timed = 0;
+  }
+  ctx->timing = on != 0;
+  return XPIR_B200_OK;
+}
+
+int xpir_b200_ctx_kernel_time(xpir_b200_ctx *ctx, double *reply_ms, uint64_t *reply_launches, double *import_ms,
+                              uint64_t *import_launches) {
+  if (!ctx) return XPIR_B200_ERR_ARG;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  for (uint32_t l = 0; l < XPIR_B200_MAX_LEVELS; l++) {
+    if (reply_ms) reply_ms[l] = ctx->reply_ms[l];
+    if (reply_launches) reply_launches[l] = ctx->reply_timed[l];
+  }
+  if (import_ms) *import_ms = ctx->import_ms;
+  if (import_launches) *import_launches = ctx->import_timed;
   return XPIR_B200_OK;
 }
 
@@ -347,6 +394,17 @@ int xpir_b200_reply(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, cons
   const uint64_t *in = db->d_polys;
   uint64_t in_real = db->n_agg;
   *ctx->status_host = 0;
+  // Event pairs of this call (kernel timing): [2*lvl] the level's reply, [2*lvl+1] the
+  // re-import after it; a pair is read only when its launch was recorded.
+  bool timed[2 * XPIR_B200_MAX_LEVELS] = {};
+  auto time_begin = [&](uint32_t k) -> cudaError_t {
+    return ctx->timing ? cudaEventRecord(ctx->timing_ev[k][0], ctx->stream) : cudaSuccess;
+  };
+  auto time_end = [&](uint32_t k, uint32_t launched) -> cudaError_t {
+    if (!ctx->timing || launched == 0) return cudaSuccess;
+    timed[k] = true;
+    return cudaEventRecord(ctx->timing_ev[k][1], ctx->stream);
+  };
   for (uint32_t lvl = 0; lvl < d; lvl++) {
     const bool last = lvl + 1 == d;
     uint64_t *rep = (last && out_on_device) ? (uint64_t *)replies : (uint64_t *)ctx->ws_a;
@@ -355,10 +413,12 @@ int xpir_b200_reply(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, cons
     a.write_idle = last;
     a.wait_test = ctx->wait_test;
     const uint64_t active = active_groups(in_real, n[lvl], groups[lvl]);
+    XPIR_TRY(time_begin(2 * lvl));
     const cudaError_t le = launch_reply_level(a, ps, dm, ctx->stream, &launched, ctx->status_dev,
                                               tuned_tile(ctx, Ps[lvl], n[lvl], groups[lvl]));
     if (le == cudaErrorNotSupported) return XPIR_B200_ERR_ARG;
     XPIR_TRY(le);
+    XPIR_TRY(time_end(2 * lvl, launched));
     ctx->launches += launched;
     dq += (uint64_t)n[lvl] * ct_words;
     if (last) break;
@@ -368,8 +428,10 @@ int xpir_b200_reply(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, cons
     const AggSource as{(const uint8_t *)rep, groups[lvl], Ps[lvl] * ct_bytes, Ps[lvl] * ct_bytes, 1};
     const ImportRows rows{1, groups[lvl], active};
     launched = 0;
+    XPIR_TRY(time_begin(2 * lvl + 1));
     XPIR_TRY(launch_import(as, groups[lvl], Ps[lvl + 1], ps, dm, ctx->d_tables, (uint64_t *)ctx->ws_b,
                            ctx->stream, &rows, &launched));
+    XPIR_TRY(time_end(2 * lvl + 1, launched));
     ctx->launches += launched;
     in = (const uint64_t *)ctx->ws_b;
     in_real = groups[lvl];
@@ -377,6 +439,18 @@ int xpir_b200_reply(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, cons
   if (!out_on_device)
     XPIR_TRY(cudaMemcpyAsync(replies, ctx->ws_a, final_bytes, cudaMemcpyDeviceToHost, ctx->stream));
   XPIR_TRY(cudaStreamSynchronize(ctx->stream));
+  for (uint32_t k = 0; k < 2 * d; k++) {
+    if (!timed[k]) continue;
+    float ms = 0;
+    XPIR_TRY(cudaEventElapsedTime(&ms, ctx->timing_ev[k][0], ctx->timing_ev[k][1]));
+    if (k % 2 == 0) {
+      ctx->reply_ms[k / 2] += ms;
+      ctx->reply_timed[k / 2]++;
+    } else {
+      ctx->import_ms += ms;
+      ctx->import_timed++;
+    }
+  }
   if (*(volatile int *)ctx->status_host != 0) return XPIR_B200_ERR_TIMEOUT;
   if (nb_replies) *nb_replies = final_count;
   return XPIR_B200_OK;

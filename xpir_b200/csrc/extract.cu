@@ -227,13 +227,13 @@ extern "C" int xpir_b200_extract(xpir_b200_ctx *ctx, const uint64_t *secret_key,
     cudaFreeAsync(d_res, st);
     cudaFreeAsync(d_out, st);
   };
-  e = cudaMallocAsync((void **)&d_sk, mN * 8, st);
-  if (e == cudaSuccess) e = cudaMallocAsync((void **)&d_sks, mN * 8, st);
+  e = cudaMallocFromPoolAsync((void **)&d_sk, mN * 8, ctx->pool, st);
+  if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void **)&d_sks, mN * 8, ctx->pool, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_sk, secret_key, mN * 8, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_sks, sks.data(), mN * 8, cudaMemcpyHostToDevice, st);
   const uint64_t *level_in = (const uint64_t *)replies;
   if (e == cudaSuccess && !replies_on_device) {
-    e = cudaMallocAsync((void **)&d_in, top * ct_words * 8, st);
+    e = cudaMallocFromPoolAsync((void **)&d_in, top * ct_words * 8, ctx->pool, st);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(d_in, replies, top * ct_words * 8, cudaMemcpyHostToDevice, st);
     level_in = d_in;
@@ -247,8 +247,8 @@ extern "C" int xpir_b200_extract(xpir_b200_ctx *ctx, const uint64_t *secret_key,
     // next level as its ciphertexts: size it for both.
     uint64_t out_words = nbr * abs_words + 3;
     if (lvl > 1) out_words = std::max<uint64_t>(out_words, extract_count(aggregated_bytes, lvl - 1, bits, N, m) * ct_words);
-    e = cudaMallocAsync((void **)&res, nbr * mN * 8, st);
-    if (e == cudaSuccess) e = cudaMallocAsync((void **)&out, out_words * 8, st);
+    e = cudaMallocFromPoolAsync((void **)&res, nbr * mN * 8, ctx->pool, st);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void **)&out, out_words * 8, ctx->pool, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(out, 0, out_words * 8, st);
     if (e == cudaSuccess && nbr > 0x7fffffffull) e = cudaErrorInvalidValue;
     if (e == cudaSuccess) {

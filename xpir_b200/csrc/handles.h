@@ -15,6 +15,7 @@
 
 #include "kernels.h"
 #include "params.h"
+#include "xpir_b200.h"
 
 struct xpir_b200_db;
 struct BatchPlan;  // batch.cu
@@ -39,12 +40,22 @@ struct xpir_b200_ctx {
   void *tasks_dev = nullptr;   // task table of uncaptured batches (device copy)
   void *tasks_host = nullptr;  // and its pinned staging copy
   size_t tasks_cap = 0;        // entries of both
+  // Stream-ordered pool of the client-side entry points' per-call buffers (query
+  // generation, extraction): it keeps freed memory for the next call (release threshold
+  // UINT64_MAX), so that a call after the first maps no new device memory.
+  cudaMemPool_t pool = nullptr;
   int *status_host = nullptr;  // kernel status word (mapped pinned memory)
   int *status_dev = nullptr;
   std::set<xpir_b200_db *> dbs;  // databases imported through this context
   TuneTable tuned;
   uint64_t tune_epoch = 0;  // bumped by every autotune (invalidates captured batches)
   xpir::WaitTest wait_test;  // test support of the bounded waits (xpir_b200_ctx_set_wait_test)
+  // Kernel timing (xpir_b200_ctx_set_kernel_timing): an event pair around each level's
+  // reply launch and each re-import of xpir_b200_reply, summed after the call's sync.
+  bool timing = false;
+  cudaEvent_t timing_ev[2 * XPIR_B200_MAX_LEVELS][2] = {};
+  double reply_ms[XPIR_B200_MAX_LEVELS] = {}, import_ms = 0;
+  uint64_t reply_timed[XPIR_B200_MAX_LEVELS] = {}, import_timed = 0;
   std::vector<std::shared_ptr<BatchPlan>> plans;  // captured batches (batch.cu)
 };
 

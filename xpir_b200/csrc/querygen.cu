@@ -7,13 +7,16 @@
 // ciphertext t of a query uses nonces first + 2t and first + 2t + 1; Salsa20 being a
 // counter-mode stream, every 64-byte block is computed independently on the device.
 //
-// encrypt_kernel: one CTA per (ciphertext, modulus):
-//   e   = noise word & mask, minus the bound when above it, amplified by 2^b mod p
-//         (Shoup), plus the plaintext bit on the constant coefficient;
-//   b   = NTT(phi-twist(e + m)) with the import's lazy NTT;
-//   a   = uniform word & mask, minus p when above it;
-//   b  += a*s (lazy Shoup MAC), then both halves fully reduced (SHOUP is defined in the
-//         reference, crypto/NFLLWE.hpp:21, crypto/NFLLWE.cpp:355-358).
+// encrypt_kernel: one CTA per ciphertext.  The noise is drawn once (its words are below
+// the noise bound, so they are kept as 32-bit words in shared memory) and serves every
+// modulus; then per modulus:
+//   e   = noise word amplified by 2^b mod p (Shoup), plus the plaintext bit on the
+//         constant coefficient;
+//   b   = NTT(phi-twist(e + m)) with the import's lazy NTT (outputs in [0, 2p));
+//   a   = uniform word & mask, minus p when above it (so a < p);
+//   b  += a*s (lazy Shoup MAC: [0, 3p)), then both halves fully reduced (SHOUP is defined
+//         in the reference, crypto/NFLLWE.hpp:21, crypto/NFLLWE.cpp:355-358): a already
+//         is, b by two conditional subtractions (2p, then p), which is b mod p for b < 4p.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
@@ -86,51 +89,65 @@ __device__ __forceinline__ void salsa20_block(const uint32_t key[8], uint64_t no
   for (int i = 0; i < 16; i++) out[i] = x[i] + in[i];
 }
 
-__global__ void __launch_bounds__(256) encrypt_kernel(const QueryGenArgs g, const uint64_t *__restrict__ sk,
+__global__ void __launch_bounds__(256, 4) encrypt_kernel(const QueryGenArgs g, const uint64_t *__restrict__ sk,
                                                       const uint64_t *__restrict__ sks,
                                                       const uint64_t *__restrict__ tables, uint32_t N, uint32_t log_n,
                                                       uint32_t m, const DevModuli dm, uint64_t *__restrict__ out) {
-  extern __shared__ uint64_t poly[];
+  extern __shared__ uint64_t poly[];                     // N words, swizzled (the NTT's buffer)
+  uint32_t *noise = reinterpret_cast<uint32_t *>(poly + N);  // N words, [k][blk] (conflict-free)
+  const uint32_t nb = N / 8;                             // Salsa20 blocks of 8 words per poly
   const uint64_t t = blockIdx.x;
-  const uint32_t c = blockIdx.y;
-  const uint64_t p = dm.p[c];
   uint64_t ui = 0;
   for (uint32_t l = 0; l < g.d; l++) ui |= (g.one_slot[l] == t) ? 1 : 0;
-  const uint64_t *tab = tables + (uint64_t)c * kTableSlots * N;
-  const uint64_t *phi = tab + kPhi * N, *phis = tab + kPhiShoup * N;
   const uint64_t nonce_e = g.first_nonce + 2 * t, nonce_a = nonce_e + 1;
-  // noise e (the same words for every modulus), amplified, plus the plaintext, twisted
-  for (uint32_t blk = threadIdx.x; blk < N / 8; blk += blockDim.x) {
+  // noise e (the same words for every modulus): word & mask, minus the bound when above it
+  for (uint32_t blk = threadIdx.x; blk < nb; blk += blockDim.x) {
     uint32_t w[16];
     salsa20_block(g.key, nonce_e, blk, w);
 #pragma unroll
     for (int k = 0; k < 8; k++) {
-      const uint32_t i = blk * 8 + k;
       uint64_t r = ((uint64_t)w[2 * k] | (uint64_t)w[2 * k + 1] << 32) & g.noise_mask;
       if (r >= g.noise_bound) r -= g.noise_bound;
-      uint64_t z = shoup_mul(r, g.amp[c], g.amp_shoup[c], p) + (i == 0 ? ui : 0);
-      z -= (z >= p) ? p : 0;
-      if (z > p) z -= p;
-      poly[swz(i)] = shoup_mul(z, phi[i], phis[i], p);
+      noise[k * nb + blk] = (uint32_t)r;  // read back by this thread only
     }
   }
-  __syncthreads();
-  ntt_lazy_rb<3>(poly, tab + kOmega * N, tab + kOmegaShoup * N, N, log_n, p, [&](uint32_t k) { return poly[swz(k)]; });
-  // uniform a: words [c*N, (c+1)*N) of the second call's stream
-  uint64_t *a_out = out + (t * 2 * m + c) * N, *b_out = out + (t * 2 * m + m + c) * N;
-  const uint64_t *s = sk + (uint64_t)c * N, *ss = sks + (uint64_t)c * N;
-  for (uint32_t blk = threadIdx.x; blk < N / 8; blk += blockDim.x) {
-    uint32_t w[16];
-    salsa20_block(g.key, nonce_a, (uint64_t)c * (N / 8) + blk, w);
+  for (uint32_t c = 0; c < m; c++) {
+    const uint64_t p = dm.p[c], p2 = p << 1;
+    const uint64_t *tab = tables + (uint64_t)c * kTableSlots * N;
+    const uint64_t *phi = tab + kPhi * N, *phis = tab + kPhiShoup * N;
+    // amplified, plus the plaintext, twisted
+    for (uint32_t blk = threadIdx.x; blk < nb; blk += blockDim.x) {
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-      const uint32_t i = blk * 8 + k;
-      uint64_t a = ((uint64_t)w[2 * k] | (uint64_t)w[2 * k + 1] << 32) & g.uniform_mask[c];
-      if (a >= p) a -= p;
-      const uint64_t b = shoup_mac(poly[swz(i)], a, s[i], ss[i], p);
-      a_out[i] = a % p;
-      b_out[i] = b % p;
+      for (int k = 0; k < 8; k++) {
+        const uint32_t i = blk * 8 + k;
+        uint64_t z = shoup_mul(noise[k * nb + blk], g.amp[c], g.amp_shoup[c], p) + (i == 0 ? ui : 0);
+        z -= (z >= p) ? p : 0;
+        if (z > p) z -= p;
+        poly[swz(i)] = shoup_mul(z, phi[i], phis[i], p);
+      }
     }
+    __syncthreads();
+    ntt_lazy_rb<3>(poly, tab + kOmega * N, tab + kOmegaShoup * N, N, log_n, p,
+                   [&](uint32_t k) { return poly[swz(k)]; });
+    // uniform a: words [c*N, (c+1)*N) of the second call's stream
+    uint64_t *a_out = out + (t * 2 * m + c) * N, *b_out = out + (t * 2 * m + m + c) * N;
+    const uint64_t *s = sk + (uint64_t)c * N, *ss = sks + (uint64_t)c * N;
+    for (uint32_t blk = threadIdx.x; blk < nb; blk += blockDim.x) {
+      uint32_t w[16];
+      salsa20_block(g.key, nonce_a, (uint64_t)c * nb + blk, w);
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const uint32_t i = blk * 8 + k;
+        uint64_t a = ((uint64_t)w[2 * k] | (uint64_t)w[2 * k + 1] << 32) & g.uniform_mask[c];
+        if (a >= p) a -= p;
+        uint64_t b = shoup_mac(poly[swz(i)], a, s[i], ss[i], p);
+        b -= (b >= p2) ? p2 : 0;
+        b -= (b >= p) ? p : 0;
+        a_out[i] = a;
+        b_out[i] = b;
+      }
+    }
+    __syncthreads();  // the next modulus rewrites poly
   }
 }
 
@@ -198,6 +215,7 @@ extern "C" int xpir_b200_generate_query(xpir_b200_ctx *ctx, const uint8_t *prng_
   }
   g.noise_bound = 2 * (5 * (uint64_t)security_bits / 2) - 1;  // 2*Berr - 1, Berr = 5k/2 (NFLLWE.cpp:83)
   g.noise_mask = bound_mask(g.noise_bound);
+  if (g.noise_mask >= (1ULL << 32)) return XPIR_B200_ERR_ARG;  // the kernel keeps noise words in 32 bits
   for (uint32_t c = 0; c < m; c++) {
     const uint64_t p = ps.mod[c].p;
     g.amp[c] = (uint64_t)((((unsigned __int128)1) << bits_per_coeff) % p);  // 2^b mod p (NFLLWE.cpp:590-604)
@@ -215,20 +233,19 @@ extern "C" int xpir_b200_generate_query(xpir_b200_ctx *ctx, const uint8_t *prng_
   if (e != cudaSuccess) return status_of(e);
   cudaStream_t st = ctx->stream;
   uint64_t *d_sk = nullptr, *d_sks = nullptr, *d_out = nullptr;
-  e = cudaMallocAsync((void **)&d_sk, mN * 8, st);
-  if (e == cudaSuccess) e = cudaMallocAsync((void **)&d_sks, mN * 8, st);
+  e = cudaMallocFromPoolAsync((void **)&d_sk, mN * 8, ctx->pool, st);
+  if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void **)&d_sks, mN * 8, ctx->pool, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_sk, secret_key, mN * 8, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_sks, sks.data(), mN * 8, cudaMemcpyHostToDevice, st);
   uint64_t *target = (uint64_t *)query;
   if (e == cudaSuccess && !out_on_device) {
-    e = cudaMallocAsync((void **)&d_out, nq * ct_bytes, st);
+    e = cudaMallocFromPoolAsync((void **)&d_out, nq * ct_bytes, ctx->pool, st);
     target = d_out;
   }
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(encrypt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(N * 8));
+  const int smem = (int)(N * 8 + N * 4);  // the NTT's poly and the 32-bit noise words
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(encrypt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e == cudaSuccess) {
-    encrypt_kernel<<<dim3((unsigned)nq, m), 256, N * 8, st>>>(g, d_sk, d_sks, ctx->d_tables, N, ps.log_n, m, dm,
-                                                              target);
+    encrypt_kernel<<<(unsigned)nq, 256, smem, st>>>(g, d_sk, d_sks, ctx->d_tables, N, ps.log_n, m, dm, target);
     e = cudaGetLastError();
     ctx->launches++;
   }
@@ -258,7 +275,7 @@ extern "C" int xpir_b200_generate_secret_key(xpir_b200_ctx *ctx, const uint8_t *
   if (e != cudaSuccess) return status_of(e);
   cudaStream_t st = ctx->stream;
   uint64_t *d_sk = nullptr;
-  e = cudaMallocAsync((void **)&d_sk, mN * 8, st);
+  e = cudaMallocFromPoolAsync((void **)&d_sk, mN * 8, ctx->pool, st);
   if (e == cudaSuccess) {
     keygen_kernel<<<dim3((ps.N / 8 + 255) / 256, ps.m), 256, 0, st>>>(g, nonce, ps.N, dm, d_sk);
     e = cudaGetLastError();
