@@ -80,6 +80,10 @@ WORKLOADS = {
 }
 
 
+for _name, _w in WORKLOADS.items():
+    _w["name"] = _name
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -188,9 +192,13 @@ def synthetic_query(seed: int, n: list[int], N: int, m: int, moduli: list[int], 
 def run_reference(w: dict, steps: int, warmup: int, threads: int) -> dict:
     """The XPIR reference (oracle/_ref) answering `steps` queries after `warmup` untimed
     ones, on one import of the workload: the full workload, except where the reference's
-    host memory for the zero-padding slots of the index grid rules it out (the recursive
-    workload: about 103 GB), where it takes `sample` elements on the same grid shape and
-    the reply time is scaled to the full database."""
+    host memory for the index grid rules it out (the recursive workload: its zero-padding
+    slots take about 103 GB), where it takes `sample` elements on the same grid.  The
+    reference pads the grid with zero polys (PIRReplyGeneratorNFL_internal.cpp:146-154) and
+    its reply loop multiplies every slot, padding included (:540-560), so on the same grid
+    its reply does the same work whatever the share of real elements: the sample's reply
+    time stands for the full workload's, unscaled.  (Zero slots may run a little faster
+    than real ones, which makes this estimate of the reference's time a lower bound.)"""
     from oracle import pyoracle as po
 
     if not po.ref_available():
@@ -206,12 +214,20 @@ def run_reference(w: dict, steps: int, warmup: int, threads: int) -> dict:
     imported = r["nb_elements"] * r["polys_per_element"] * w["m"] * w["N"] * 8
     reply_s = statistics.mean(r["reply_s"])
     full_imported = imported * w["F"] / S
-    full_reply_s = reply_s * w["F"] / S
+    # d = 1: the sample's grid is the sample (time scales with it); d > 1: the same grid.
+    full_reply_s = reply_s * w["F"] / S if len(n) == 1 else reply_s
     return {"value": full_imported / full_reply_s / 1e9, "reply_s": reply_s, "full_reply_s": full_reply_s,
             "reply_s_all": r["reply_s"], "import_s": r["import_s"], "import_gbs": imported / r["import_s"] / 1e9,
             "imported_bytes": imported, "elements": S, "same_config": S == w["F"], "n": n,
             "threads": r["omp_threads"], "bits_per_coeff": r["bits_per_coeff"],
             "polys_per_element": r["polys_per_element"], "cpu_model": po.host_cpu_model()}
+
+
+def sample_words(r: dict, w: dict) -> str:
+    if len(w["n"]) > 1:
+        return (f"{r['elements']} of {w['F']} elements on the full {'x'.join(map(str, w['n']))} grid (reply time "
+                f"unscaled: the reference multiplies every grid slot, zero padding included)")
+    return f"{r['elements']} of {w['F']} elements (reply time scaled by {w['F']}/{r['elements']})"
 
 
 def reference_arm(args, w: dict, world: int, rank: int) -> int:
@@ -222,7 +238,7 @@ def reference_arm(args, w: dict, world: int, rank: int) -> int:
     if "unavailable" in r:
         print(json.dumps({"impl": "reference", "unavailable": r["unavailable"]}))
         return 0
-    sample = (f"{'the full workload' if r['same_config'] else str(r['elements']) + ' elements (scaled)'} "
+    sample = (f"{'the full workload' if r['same_config'] else sample_words(r, w)} "
               f"(n={r['n']}, bits/coeff {r['bits_per_coeff']}): one import, {args.steps} timed replies after "
               f"{args.warmup} untimed, each timed with omp_get_wtime at the reference's own boundaries")
     line = {
@@ -246,9 +262,41 @@ def reference_arm(args, w: dict, world: int, rank: int) -> int:
 def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
     import torch
 
+    dist = init_dist(world, local)
+    line = measure_single(args, w, world, rank, local, dist)
+    torch.cuda.empty_cache()
+    # The rest of the metric, on the same GPU after the single query's buffers are freed:
+    # batched vs plain queries/s (every rank, as replicas), the serving loop's p50/p99
+    # latency (one GPU: a server answers on the GPU it runs on), and the reference's other
+    # two single-query configurations (plain and recursive) as replicas.
+    if args.extras and args.workload == "memory_bound" and not args.elements:
+        b = measure_batched(args, WORKLOADS["batched"], world, rank, local, dist)
+        if rank == 0:
+            line["batched"] = sub_object(b)
+        if world == 1:
+            line["serving"] = sub_object(measure_serving(args, WORKLOADS["serving"], local))
+        elif rank == 0:
+            line["serving"] = {"skipped": "the serving loop runs on one GPU; it is measured in the N=1 run"}
+        for name in ("plain", "recursive"):
+            sub = measure_single(args, dict(WORKLOADS[name]), world, rank, local, dist)
+            torch.cuda.empty_cache()
+            if rank == 0:
+                line[name] = sub_object(sub)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def measure_single(args, w: dict, world: int, rank: int, local: int, dist) -> dict | None:
+    """One single-query workload: device-resident `value`, kernel roofline, e2e through the
+    C ABI with host buffers, and (N = 1) the reference's CPU reply beside it.  Returns the
+    result line on rank 0 (None elsewhere)."""
+    import torch
+
     import xpir_b200
 
-    dist = init_dist(world, local)
     device = local
     torch.cuda.set_device(device)
     N, m, n, alpha, F, L = w["N"], w["m"], w["n"], w["alpha"], w["F"], w["L"]
@@ -362,7 +410,7 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
             # measured bytes per algorithmic byte of this kernel on this workload, applied
             # to this launch's algorithmic bytes.
             traffic = (round(algo_bytes * REPLY_TRAFFIC_PER_ALGORITHMIC_BYTE)
-                       if args.workload == "memory_bound" else None)
+                       if w["name"] == "memory_bound" else None)
             roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                         "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
                         "kernel": "reply_tma_kernel" + (" (level 1)" if len(n) > 1 else ""),
@@ -376,7 +424,7 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
         if world == 1 and not args.no_cpu_baseline:
             r = run_reference(w, steps=1, warmup=0, threads=os.cpu_count() or 1)
             if "unavailable" not in r:
-                what = "the full workload" if r["same_config"] else f"{r['elements']} of {F} elements (scaled)"
+                what = "the full workload" if r["same_config"] else sample_words(r, w)
                 cpu = {"value": round(r["value"], 4), "unit": "GB/s", "cores": r["threads"], "kind": "reference",
                        "cpu_model": r["cpu_model"],
                        "sample": (f"{what} (n={r['n']}); one reference reply {r['reply_s']:.3f} s, import "
@@ -405,23 +453,7 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
     dbh.free()
     ctx.close()
     del q_dev, q_host, out_dev, out_host, flush_buf
-    torch.cuda.empty_cache()
-    # The rest of the metric, on the same GPU after the single query's buffers are freed:
-    # batched vs plain queries/s (every rank, as replicas) and the serving loop's p50/p99
-    # latency (one GPU: a server answers on the GPU it runs on).
-    if args.extras and args.workload == "memory_bound" and not args.elements:
-        b = measure_batched(args, WORKLOADS["batched"], world, rank, local, dist)
-        if rank == 0:
-            line["batched"] = sub_object(b)
-        if world == 1:
-            line["serving"] = sub_object(measure_serving(args, WORKLOADS["serving"], local))
-        elif rank == 0:
-            line["serving"] = {"skipped": "the serving loop runs on one GPU; it is measured in the N=1 run"}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
-    return 0
+    return line
 
 
 def sub_object(line: dict) -> dict:
