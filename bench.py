@@ -40,11 +40,13 @@ sys.path.insert(0, str(ROOT))
 METRIC = "reply-gen DB GB/s vs HBM peak; batched vs plain queries/s; p50/p99 latency"
 
 # dram__bytes_read.sum + dram__bytes_write.sum over the algorithmic bytes (DB + query +
-# reply) of one reply_tma_kernel launch on the memory-bound workload, from one
-# `ncu --set full` capture of a 10,000-element case of the same kernel and grid
-# (traffic grows with the elements: each is one DB row and one query ciphertext):
-# (995.5 + 3.7) MB / 983.1 MB.
-REPLY_TRAFFIC_PER_ALGORITHMIC_BYTE = 1.0164
+# replies) of one first-level reply_tma_kernel launch, per workload, each from one
+# `ncu --set full` capture of a smaller case of the same kernel and tile (traffic grows
+# with the elements: each is one DB row and its share of the query):
+#   memory_bound: 10,000 elements, (995.5 + 3.7) MB / 983.1 MB;
+#   recursive:    262,144 elements (16 groups), (1,823 + 6.7) MB / (1,811.9 + 3.1) MB;
+#   plain:        the full workload (L2 flushed before the launch), (73.8 + 1.7) MB / 73.8 MB.
+REPLY_TRAFFIC_PER_ALGORITHMIC_BYTE = {"memory_bound": 1.0164, "recursive": 1.0081, "plain": 1.0219}
 
 WORKLOADS = {
     # name: N, m, n levels, alpha, elements, element bytes, chosen index, cpu-sample elements
@@ -409,8 +411,8 @@ def measure_single(args, w: dict, world: int, rank: int, local: int, dist) -> di
             # DRAM traffic cannot be read without a profiler: it is the ncu capture's
             # measured bytes per algorithmic byte of this kernel on this workload, applied
             # to this launch's algorithmic bytes.
-            traffic = (round(algo_bytes * REPLY_TRAFFIC_PER_ALGORITHMIC_BYTE)
-                       if w["name"] == "memory_bound" else None)
+            ratio = REPLY_TRAFFIC_PER_ALGORITHMIC_BYTE.get(w["name"])
+            traffic = round(algo_bytes * ratio) if ratio else None
             roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                         "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
                         "kernel": "reply_tma_kernel" + (" (level 1)" if len(n) > 1 else ""),
