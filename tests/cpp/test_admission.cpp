@@ -9,7 +9,9 @@
 //   6. a head-of-line job that does not fit waits for memory rather than being skipped;
 //   7. as a two-stage pipeline (depth 2), stage 1 of a lane's next batch overlaps stage 2
 //      of its current one, at most two batches per lane are in flight, stage 2 sees the
-//      batches in admission order, and every job completes.
+//      batches in admission order, and every job completes;
+//   8. a job waiting for memory at the head of one lane is not overtaken by jobs submitted
+//      after it on another lane.
 #include <stdio.h>
 
 #include <atomic>
@@ -126,6 +128,31 @@ int main() {
   adm.release(a);
   adm.release(big);
   adm.release(small);
+
+  // 8. Across lanes: a job needing the whole budget at the head of lane 0 is not starved
+  // by jobs submitted after it on lanes 1 and 2, whose batches would otherwise overlap so
+  // that the budget never empties: none of them is admitted before it.
+  {
+    Admission three(3, budget, 1, [&](uint32_t, std::vector<Job *> &batch) {
+      std::this_thread::sleep_for(std::chrono::milliseconds(15));
+      for (Job *j : batch) j->status = 0;
+    });
+    const uint64_t a1 = three.submit(1, 300, nullptr);
+    std::this_thread::sleep_for(std::chrono::milliseconds(7));  // staggered: the lanes' batches interleave
+    const uint64_t a2 = three.submit(2, 300, nullptr);
+    std::this_thread::sleep_for(std::chrono::milliseconds(2));
+    const uint64_t whole = three.submit(0, budget, nullptr);
+    std::vector<uint64_t> later;
+    for (int i = 0; i < 10; i++) later.push_back(three.submit(1 + i % 2, 300, nullptr));
+    Job *jw = three.wait(whole, 20000);
+    CHECK(a1 && a2 && jw);
+    for (uint64_t t : later) {
+      Job *j = three.wait(t, 20000);
+      CHECK(j && j->t_admit >= jw->t_admit);
+    }
+    CHECK(three.stats().peak_in_use <= budget);
+    three.stop();
+  }
 
   // Timeout: a job that cannot finish within the wait's limit.
   delay_ms = 300;

@@ -101,3 +101,26 @@ def test_oversize_query_refused(engine):
             with pytest.raises(engine.XpirError) as ei:
                 srv.submit(db, [F], q, out)
             assert ei.value.status == engine.ERR_NOMEM
+
+
+def test_large_pinned_query_is_pulled_and_exact(engine):
+    """A query of 256 MB or more in pinned host memory is pulled over PCIe by the server's
+    copy kernel instead of the copy engine; pageable queries of the same size take the copy
+    engine.  Both replies equal the reply computed alone, and small queries served beside
+    them too."""
+    import torch
+
+    N, m, F, L = 2048, 2, 4500, 4096
+    n = [F]  # 4,500 ciphertexts of 64 KB: 295 MB of query
+    b = engine.bits_per_coeff(N, m, n[0])
+    with engine.Context(1024, 1) as ca, engine.Context(N, m) as cb:
+        db = cb.import_db(random_db(91, F, L), F, L, 1, b)
+        q = random_query(92, n, N, m, engine.moduli(m))
+        want = cb.reply(db, n, q)
+        pinned = torch.from_numpy(q.view(np.int64)).pin_memory()
+        small, _ = make_load(engine, [(ca, (1024, 1)), (cb, (2048, 2))])
+        with engine.Server([ca, cb], device_budget_bytes=4 << 30, max_batch=16) as srv:
+            big = [(db, n, pinned.numpy().view(np.uint64), want), (db, n, q, want)]
+            outs, _ = serve_all(engine, srv, big + small, clients=3)
+        for (_, _, _, w), got in zip(big + small, outs):
+            assert np.array_equal(got, w)

@@ -2,7 +2,10 @@
 //
 // Requests wait in FIFO order per lane.  A lane's worker takes the longest prefix of its
 // queue whose device-memory footprints fit in what the shared budget has left (at most
-// max_batch requests), runs them as one batch, then releases their memory.  Requests
+// max_batch requests), runs them as one batch, then releases their memory.  The memory
+// of the other lanes' heads that arrived earlier is kept for them: a request is admitted
+// only if it fits beside those heads, so a large request at the head of one lane is not
+// starved by a stream of later small ones on the others.  Requests
 // that arrive while a batch runs wait for the next one; a request larger than the whole
 // budget is refused at submission.  The executor (the GPU in the server, a fake in the
 // CPU tests) is a callback.
@@ -141,11 +144,11 @@ class Admission {
       cv_.wait(lk, [&] {
         if (stopping_) return true;
         auto &q = queues_[lane];
-        return inflight_[lane] < depth_ && !q.empty() && q.front()->footprint <= budget_ - in_use_;
+        return inflight_[lane] < depth_ && !q.empty() && fits(lane, q.front());
       });
       if (stopping_) return;
       auto &q = queues_[lane];
-      while (!q.empty() && batch.size() < max_batch_ && q.front()->footprint <= budget_ - in_use_) {
+      while (!q.empty() && batch.size() < max_batch_ && fits(lane, q.front())) {
         Job *j = q.front();
         q.pop_front();
         in_use_ += j->footprint;
@@ -164,6 +167,21 @@ class Admission {
         complete(lane, batch);
       }
     }
+  }
+
+  // With mu_ held: whether job j of `lane` fits in the budget left beside the footprints
+  // of the other lanes' heads that were submitted before it.
+  bool fits(uint32_t lane, const Job *j) const {
+    uint64_t need = j->footprint;
+    for (uint32_t l = 0; l < queues_.size(); l++) {
+      if (l == lane || queues_[l].empty()) continue;
+      const Job *h = queues_[l].front();
+      if (h->ticket < j->ticket) {
+        if (need > budget_ - h->footprint) return false;  // more than the whole budget
+        need += h->footprint;
+      }
+    }
+    return need <= budget_ - in_use_;
   }
 
   // Stage 2 of a pipelined lane: in admission order, and drained before stop returns.
