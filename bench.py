@@ -276,7 +276,13 @@ def ours_arm(args, w: dict, world: int, rank: int, local: int) -> int:
         if rank == 0:
             line["batched"] = sub_object(b)
         if world == 1:
-            line["serving"] = sub_object(measure_serving(args, WORKLOADS["serving"], local))
+            # One GPU, no collective: a failure here is reported in the line, beside the
+            # measurements already taken, instead of ending the run.
+            try:
+                line["serving"] = sub_object(measure_serving(args, WORKLOADS["serving"], local))
+            except Exception as exc:  # noqa: BLE001 - recorded, not hidden
+                line["serving"] = {"error": f"{type(exc).__name__}: {exc}"}
+                log(f"serving failed: {exc}")
         elif rank == 0:
             line["serving"] = {"skipped": "the serving loop runs on one GPU; it is measured in the N=1 run"}
         for name in ("plain", "recursive"):
@@ -810,6 +816,8 @@ def measure_serving(args, w: dict, local: int) -> dict:
     device = local
     torch.cuda.set_device(device)
     dev = f"cuda:{device}"
+    free, total = torch.cuda.mem_get_info(device)
+    log(f"serving: {free / 1e9:.1f} of {total / 1e9:.1f} GB free on the device")
     shapes = serving_shapes(w)
     ctxs = [xpir_b200.Context(N, m, device=device) for (_, N, m, _, _) in w["dbs"]]
     # Imports: one per (database, alpha, bits per coefficient), from device-resident bytes.

@@ -46,7 +46,8 @@ typedef struct xpir_b200_db xpir_b200_db;   /* an imported database resident in 
 /* ---- library ------------------------------------------------------------------ */
 XPIR_B200_API const char *xpir_b200_version(void);
 XPIR_B200_API const char *xpir_b200_strerror(int status);
-/* Name of the last CUDA error seen by any call (diagnostics). */
+/* Name of the last CUDA error seen by the calling thread's calls (diagnostics); for a
+ * served query, xpir_b200_server_wait reports the query's CUDA error to its caller. */
 XPIR_B200_API const char *xpir_b200_last_cuda_error(void);
 XPIR_B200_API int xpir_b200_device_count(int *count);
 

@@ -228,6 +228,7 @@ int xpir::reply_batch_impl(xpir_b200_ctx *ctx, xpir_b200_request *reqs, uint32_t
   auto finish = [&](cudaError_t err) -> int {
     const cudaError_t se = cudaStreamSynchronize(ctx->stream);  // also on error: nothing left in flight
     if (err == cudaSuccess) err = se;
+    if (err != cudaSuccess) ctx->last_error = err;
     int rc = status_of(err);
     if (rc == XPIR_B200_OK && *(volatile int *)ctx->status_host != 0) rc = XPIR_B200_ERR_TIMEOUT;
     for (const Group &g : groups)

@@ -64,6 +64,10 @@ ParamSet with_bits(const ParamSet &base, uint32_t b) {
 
 }  // namespace
 
+void xpir::note_cuda_error(cudaError_t e) {
+  if (e != cudaSuccess) g_last_cuda = e;
+}
+
 extern "C" {
 
 const char *xpir_b200_version(void) { return "xpir_b200 0.1 (sm_100a)"; }

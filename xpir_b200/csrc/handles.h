@@ -29,7 +29,8 @@ struct xpir_b200_ctx {
   xpir::ParamSet ps;           // b is set per database
   uint64_t *d_tables = nullptr;
   std::mutex mu;
-  uint64_t launches = 0;
+  std::atomic<uint64_t> launches{0};  // engine kernels launched (also counted off the lock)
+  cudaError_t last_error = cudaSuccess;  // the last CUDA error of a batch on this context
   // grow-only workspaces (device)
   void *ws_query = nullptr;
   size_t ws_query_bytes = 0;
@@ -77,6 +78,11 @@ struct xpir_b200_db {
 };
 
 struct xpir_b200_request;
+
+namespace xpir {
+// Records a CUDA error as the calling thread's xpir_b200_last_cuda_error().
+void note_cuda_error(cudaError_t e);
+}  // namespace xpir
 
 namespace xpir {
 

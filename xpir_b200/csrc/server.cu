@@ -35,6 +35,7 @@ struct ServedQuery {
   void *dq = nullptr, *dr = nullptr;
   cudaEvent_t uploaded = nullptr;  // on the batch's first query only
   int upload_status = 0;
+  cudaError_t cuda_error = cudaSuccess;  // the CUDA error behind an XPIR_B200_ERR_CUDA status
 };
 
 }  // namespace
@@ -107,7 +108,6 @@ void upload_batch(xpir_b200_server *srv, uint32_t lane, std::vector<xpir::Job *>
       pull_host_kernel<<<kPullBlocks, kPullThreads, 0, cs>>>((const uint4 *)mapped, (uint4 *)q->dq,
                                                             q->query_bytes / 16);
       e = cudaGetLastError();
-      std::lock_guard<std::mutex> lock(ctx->mu);
       ctx->launches++;
     } else {
       e = cudaMemcpyAsync(q->dq, q->host_query, q->query_bytes, cudaMemcpyHostToDevice, cs);
@@ -118,7 +118,11 @@ void upload_batch(xpir_b200_server *srv, uint32_t lane, std::vector<xpir::Job *>
   if (e == cudaSuccess) e = cudaEventRecord(q0->uploaded, cs);
   if (e != cudaSuccess) {
     (void)cudaGetLastError();
-    for (auto *j : batch) ((ServedQuery *)j->payload.get())->upload_status = status_of_error(e);
+    for (auto *j : batch) {
+      auto *q = (ServedQuery *)j->payload.get();
+      q->upload_status = status_of_error(e);
+      q->cuda_error = e;
+    }
   }
 }
 
@@ -160,10 +164,15 @@ void compute_batch(xpir_b200_server *srv, uint32_t lane, std::vector<xpir::Job *
   for (size_t i = 0; i < batch.size(); i++) {
     auto *q = (ServedQuery *)batch[i]->payload.get();
     int s = run ? reqs[i].status : (upload != XPIR_B200_OK ? upload : status_of_error(e));
+    if (!run && upload == XPIR_B200_OK) q->cuda_error = e;
+    if (run && s == XPIR_B200_ERR_CUDA) q->cuda_error = ctx->last_error;
     if (s == XPIR_B200_OK) {
       q->nb_replies = reqs[i].nb_replies;
-      if (cudaMemcpyAsync(q->host_replies, q->dr, q->reply_bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+      const cudaError_t ce = cudaMemcpyAsync(q->host_replies, q->dr, q->reply_bytes, cudaMemcpyDeviceToHost, st);
+      if (ce != cudaSuccess) {
         s = XPIR_B200_ERR_CUDA;
+        q->cuda_error = ce;
+      }
     }
     batch[i]->status = s;
   }
@@ -174,8 +183,12 @@ void compute_batch(xpir_b200_server *srv, uint32_t lane, std::vector<xpir::Job *
     q->dq = q->dr = nullptr;
   }
   for (void *p : held) cudaFreeAsync(p, st);
-  if (cudaStreamSynchronize(st) != cudaSuccess)
-    for (auto *j : batch) j->status = XPIR_B200_ERR_CUDA;
+  const cudaError_t se = cudaStreamSynchronize(st);
+  if (se != cudaSuccess)
+    for (auto *j : batch) {
+      j->status = XPIR_B200_ERR_CUDA;
+      ((ServedQuery *)j->payload.get())->cuda_error = se;
+    }
   if (q0->uploaded) cudaEventDestroy(q0->uploaded);
   q0->uploaded = nullptr;
 }
@@ -295,6 +308,7 @@ int xpir_b200_server_wait(xpir_b200_server *srv, uint64_t ticket, int timeout_ms
   xpir::Job *j = srv->adm->wait(ticket, timeout_ms);
   if (!j) return XPIR_B200_ERR_STATE;  // unknown ticket or not done within the timeout
   const int status = j->status;
+  if (status == XPIR_B200_ERR_CUDA) xpir::note_cuda_error(((ServedQuery *)j->payload.get())->cuda_error);
   if (nb_replies) *nb_replies = ((ServedQuery *)j->payload.get())->nb_replies;
   if (latency_s) *latency_s = j->t_done - j->t_submit;
   if (queued_s) *queued_s = j->t_admit - j->t_submit;
