@@ -76,7 +76,8 @@ XPIR_B200_API uint64_t xpir_b200_ciphertext_bytes(uint32_t poly_degree, uint32_t
  * context owns one CUDA stream; all its work is ordered on it. */
 XPIR_B200_API int xpir_b200_ctx_create(xpir_b200_ctx **ctx, int device, uint32_t poly_degree, uint32_t nb_moduli);
 /* Destroys the context and every database imported through it (their handles become
- * invalid and must not be passed to xpir_b200_db_free afterwards). */
+ * invalid and must not be passed to xpir_b200_db_free afterwards).  XPIR_B200_ERR_STATE,
+ * and nothing destroyed, while a server has a lane on the context: destroy it first. */
 XPIR_B200_API int xpir_b200_ctx_destroy(xpir_b200_ctx *ctx);
 /* The context's cudaStream_t, as a void pointer (for event timing by the caller). */
 XPIR_B200_API int xpir_b200_ctx_stream(xpir_b200_ctx *ctx, void **stream);
@@ -268,7 +269,9 @@ XPIR_B200_API int xpir_b200_server_stats(xpir_b200_server *srv, uint64_t *comple
 /* Device bytes the server reserves while one query of this shape is admitted: its query
  * and reply buffers and its share of the recursion workspace (for sizing budgets). */
 XPIR_B200_API int xpir_b200_server_footprint(const xpir_b200_db *db, uint32_t d, const uint32_t *n, uint64_t *bytes);
-/* Stops the lanes; call after every submitted query has been waited for. */
+/* Stops the lanes: admitted queries run to completion, queries still waiting for
+ * admission complete with XPIR_B200_ERR_STATE.  No xpir_b200_server_wait may be in
+ * progress or follow; the server's contexts can then be destroyed. */
 XPIR_B200_API int xpir_b200_server_destroy(xpir_b200_server *srv);
 
 /* ---- reply without allocation ---------------------------------------------------- */

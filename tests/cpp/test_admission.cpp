@@ -11,7 +11,9 @@
 //      of its current one, at most two batches per lane are in flight, stage 2 sees the
 //      batches in admission order, and every job completes;
 //   8. a job waiting for memory at the head of one lane is not overtaken by jobs submitted
-//      after it on another lane.
+//      after it on another lane;
+//   9. stopping runs the admitted jobs to completion and completes the queued ones with
+//      the cancellation status.
 #include <stdio.h>
 
 #include <atomic>
@@ -152,6 +154,22 @@ int main() {
     }
     CHECK(three.stats().peak_in_use <= budget);
     three.stop();
+  }
+
+  // 9. Stopping: the admitted job runs to completion, the queued ones complete with the
+  // cancellation status, and every waiter returns.
+  {
+    Admission one(1, budget, 1, [&](uint32_t, std::vector<Job *> &batch) {
+      std::this_thread::sleep_for(std::chrono::milliseconds(30));
+      for (Job *j : batch) j->status = 3;
+    });
+    const uint64_t t1 = one.submit(0, 10, nullptr);
+    std::this_thread::sleep_for(std::chrono::milliseconds(5));  // t1 admitted
+    const uint64_t t2 = one.submit(0, 10, nullptr), t3 = one.submit(0, 10, nullptr);
+    one.stop(-5);
+    Job *j1 = one.wait(t1, 1000), *j2 = one.wait(t2, 1000), *j3 = one.wait(t3, 1000);
+    CHECK(j1 && j2 && j3);
+    CHECK(j1->status == 3 && j2->status == -5 && j3->status == -5);
   }
 
   // Timeout: a job that cannot finish within the wait's limit.

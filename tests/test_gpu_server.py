@@ -124,3 +124,15 @@ def test_large_pinned_query_is_pulled_and_exact(engine):
             outs, _ = serve_all(engine, srv, big + small, clients=3)
         for (_, _, _, w), got in zip(big + small, outs):
             assert np.array_equal(got, w)
+
+
+def test_context_outlives_its_server(engine):
+    """A context cannot be destroyed while a server has a lane on it (the C call refuses
+    with XPIR_B200_ERR_STATE and destroys nothing); Context.close() closes the server first."""
+    lib = engine._load()
+    ctx = engine.Context(1024, 1)
+    srv = engine.Server([ctx], device_budget_bytes=1 << 28, max_batch=4)
+    assert lib.xpir_b200_ctx_destroy(ctx.handle) == engine.ERR_STATE
+    assert ctx.launch_count >= 0  # still alive
+    ctx.close()
+    assert srv.handle is None and ctx.handle is None

@@ -225,6 +225,7 @@ class Context:
         self.handle = h
         self.ct_words = 2 * m * N
         self._dbs: "weakref.WeakSet[Database]" = weakref.WeakSet()
+        self._servers: "weakref.WeakSet[Server]" = weakref.WeakSet()
 
     @property
     def stream(self) -> int:
@@ -363,6 +364,8 @@ class Context:
 
     def close(self) -> None:
         if self.handle:
+            for srv in list(self._servers):  # a server's lanes run on the context
+                srv.close()
             for db in list(self._dbs):
                 db.free()
             _check(_load().xpir_b200_ctx_destroy(self.handle), "ctx_destroy")
@@ -392,7 +395,9 @@ class Server:
         _check(_load().xpir_b200_server_create(ctypes.byref(h), arr, len(contexts), device_budget_bytes, max_batch),
                "server_create")
         self.handle = h
-        self.contexts = contexts
+        self.contexts = contexts  # kept alive while the server is
+        for c in contexts:
+            c._servers.add(self)
 
     def submit(self, db: Database, n: list[int], query, replies) -> int:
         narr = (ctypes.c_uint32 * len(n))(*n)
@@ -434,3 +439,9 @@ class Server:
 
     def __exit__(self, *exc):
         self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

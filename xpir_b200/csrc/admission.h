@@ -67,7 +67,9 @@ class Admission {
 
   ~Admission() { stop(); }
 
-  void stop() {
+  // Stops the workers once the admitted batches have completed; jobs still queued (never
+  // admitted) complete with `cancelled_status`, so that no waiter is left behind.
+  void stop(int cancelled_status = -1) {
     {
       std::lock_guard<std::mutex> lk(mu_);
       if (stopping_) return;
@@ -76,6 +78,17 @@ class Admission {
     cv_.notify_all();
     for (auto &t : workers_)
       if (t.joinable()) t.join();
+    std::lock_guard<std::mutex> lk(mu_);
+    const double t = now();
+    for (auto &q : queues_) {
+      for (Job *j : q) {
+        j->status = cancelled_status;
+        j->t_admit = j->t_done = t;
+        j->done = true;
+      }
+      q.clear();
+    }
+    done_cv_.notify_all();
   }
 
   static double now() {

@@ -8,6 +8,7 @@
 // the group's queries together.  The arithmetic per query is exactly xpir_b200_reply's.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdio.h>
 #include <string.h>
 
 #include <algorithm>
@@ -116,7 +117,11 @@ cudaError_t enqueue(xpir_b200_ctx *ctx, const std::vector<Group> &groups, const 
                                          host_tasks + task_off, dev_tasks + task_off, ctx->stream, &launched,
                                          ctx->status_dev, tuned_tile(ctx, P, g.n[lvl], groups_l), last);
       ctx->launches += launched;
-      if (e != cudaSuccess) return e;
+      if (e != cudaSuccess) {
+        fprintf(stderr, "xpir_b200: batched reply launch failed: %s (level %u of %u, P %llu, n_i %u, groups %llu, %u tasks)\n",
+                cudaGetErrorName(e), lvl, g.d, (unsigned long long)P, g.n[lvl], (unsigned long long)groups_l, k);
+        return e;
+      }
       task_off += k;
       q_off += (uint64_t)g.n[lvl] * ct_words;
       if (last) break;
@@ -128,7 +133,11 @@ cudaError_t enqueue(xpir_b200_ctx *ctx, const std::vector<Group> &groups, const 
       e = launch_import(as, (uint64_t)k * groups_l, g.sh.P[lvl + 1], ps, dm, ctx->d_tables, ws_b, ctx->stream,
                         &rows, &launched);
       ctx->launches += launched;
-      if (e != cudaSuccess) return e;
+      if (e != cudaSuccess) {
+        fprintf(stderr, "xpir_b200: batched re-import launch failed: %s (level %u of %u, %u tasks)\n",
+                cudaGetErrorName(e), lvl, g.d, k);
+        return e;
+      }
     }
   }
   return cudaSuccess;

@@ -171,6 +171,7 @@ int xpir_b200_ctx_create(xpir_b200_ctx **out, int device, uint32_t N, uint32_t m
 
 int xpir_b200_ctx_destroy(xpir_b200_ctx *ctx) {
   if (!ctx) return XPIR_B200_ERR_ARG;
+  if (ctx->servers.load() > 0) return XPIR_B200_ERR_STATE;  // a server's lane still runs on it
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (xpir_b200_db *db : ctx->dbs) {

@@ -238,8 +238,7 @@ extern "C" int xpir_b200_extract(xpir_b200_ctx *ctx, const uint64_t *secret_key,
       e = cudaMemcpyAsync(d_in, replies, top * ct_words * 8, cudaMemcpyHostToDevice, st);
     level_in = d_in;
   }
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(decrypt_poly_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)(N * 8));
+  if (e == cudaSuccess) e = allow_max_dynamic_smem((const void *)decrypt_poly_kernel);
   for (uint32_t lvl = d; lvl >= 1 && e == cudaSuccess; lvl--) {
     const uint64_t nbr = extract_count(aggregated_bytes, lvl, bits, N, m);
     uint64_t *res = nullptr, *out = nullptr;

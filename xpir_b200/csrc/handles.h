@@ -30,6 +30,7 @@ struct xpir_b200_ctx {
   uint64_t *d_tables = nullptr;
   std::mutex mu;
   std::atomic<uint64_t> launches{0};  // engine kernels launched (also counted off the lock)
+  std::atomic<int> servers{0};         // servers with a lane on this context
   cudaError_t last_error = cudaSuccess;  // the last CUDA error of a batch on this context
   // grow-only workspaces (device)
   void *ws_query = nullptr;

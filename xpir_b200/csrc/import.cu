@@ -208,7 +208,7 @@ cudaError_t launch_import(const AggSource &src, uint64_t groups, uint64_t P, con
   const uint64_t computed = r.rows * r.active, zero_polys = r.rows * (r.per_row - r.active) * P;
   if (computed * P > 0x7fffffffull) return cudaErrorInvalidValue;
   if (computed > 0) {
-    cudaError_t e = cudaFuncSetAttribute(import_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_max_dynamic_smem((const void *)import_kernel);
     if (e != cudaSuccess) return e;
     dim3 grid((unsigned)(computed * P), ps.m);
     import_kernel<<<grid, threads, smem, stream>>>(src, sh, dm, tables, out);
@@ -217,8 +217,7 @@ cudaError_t launch_import(const AggSource &src, uint64_t groups, uint64_t P, con
   }
   if (zero_polys > 0) {
     const size_t zsmem = (size_t)ps.N * sizeof(uint64_t);
-    cudaError_t e = cudaFuncSetAttribute(import_zero_fill_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)zsmem);
+    cudaError_t e = allow_max_dynamic_smem((const void *)import_zero_fill_kernel);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;

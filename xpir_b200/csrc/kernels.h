@@ -50,6 +50,14 @@ DevModuli make_dev_moduli(const ParamSet &ps);
 struct ImportRows {
   uint64_t rows, per_row, active;
 };
+
+// Lets `kernel` take up to the current device's opt-in maximum of dynamic shared memory.
+// For a kernel whose shared memory depends on the parameter set (import, extraction,
+// query generation), every caller sets this same value: contexts of different parameter
+// sets launch it from several threads, and a per-launch size set by one thread between
+// another thread's setting and launch made that launch fail (cudaErrorInvalidValue).
+cudaError_t allow_max_dynamic_smem(const void *kernel);
+
 cudaError_t launch_import(const AggSource &src, uint64_t groups, uint64_t P, const ParamSet &ps,
                           const DevModuli &dm, const uint64_t *tables, uint64_t *out, cudaStream_t stream,
                           const ImportRows *rows = nullptr, uint32_t *launches = nullptr);

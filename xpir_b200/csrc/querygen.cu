@@ -243,7 +243,7 @@ extern "C" int xpir_b200_generate_query(xpir_b200_ctx *ctx, const uint8_t *prng_
     target = d_out;
   }
   const int smem = (int)(N * 8 + N * 4);  // the NTT's poly and the 32-bit noise words
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(encrypt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess) e = allow_max_dynamic_smem((const void *)encrypt_kernel);
   if (e == cudaSuccess) {
     encrypt_kernel<<<(unsigned)nq, 256, smem, st>>>(g, d_sk, d_sks, ctx->d_tables, N, ps.log_n, m, dm, target);
     e = cudaGetLastError();

@@ -34,6 +34,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdio.h>
 
 #include <algorithm>
 
@@ -366,8 +367,12 @@ cudaError_t launch_tasks_c(const uint64_t *const *db, const uint64_t *const *que
                            uint64_t P, uint64_t groups, uint64_t n_i, const ParamSet &ps, const DevModuli &dm,
                            ReplyTask *host_tasks, ReplyTask *dev_tasks, cudaStream_t stream, int *status) {
   for (uint32_t t = 0; t < ntasks; t++) {
-    if (!encode_task<W, C, E, GRP>(db[t], query[t], n_real, P, n_i, ps, &host_tasks[t].tm_db, &host_tasks[t].tm_q))
+    if (!encode_task<W, C, E, GRP>(db[t], query[t], n_real, P, n_i, ps, &host_tasks[t].tm_db, &host_tasks[t].tm_q)) {
+      fprintf(stderr, "xpir_b200: tensor maps refused for task %u (database %p, query %p, %llu real, P %llu, n_i %llu)\n",
+              t, (const void *)db[t], (const void *)query[t], (unsigned long long)n_real, (unsigned long long)P,
+              (unsigned long long)n_i);
       return cudaErrorInvalidValue;
+    }
     host_tasks[t].out = out[t];
   }
   cudaError_t e = cudaMemcpyAsync(dev_tasks, host_tasks, ntasks * sizeof(ReplyTask), cudaMemcpyHostToDevice, stream);

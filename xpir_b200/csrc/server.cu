@@ -9,6 +9,7 @@
 // streams replies as they appear (apps/server/PIRSession.cpp:467-565).
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdio.h>
 #include <string.h>
 
 #include <algorithm>
@@ -48,6 +49,11 @@ struct xpir_b200_server {
 };
 
 namespace {
+
+// A CUDA error of a served batch, on stderr (the query's status carries it too).
+void report(const char *where, uint32_t lane, cudaError_t e) {
+  fprintf(stderr, "xpir_b200 server: %s failed on lane %u: %s\n", where, lane, cudaGetErrorName(e));
+}
 
 int status_of_error(cudaError_t e) {
   return e == cudaErrorMemoryAllocation ? XPIR_B200_ERR_NOMEM : XPIR_B200_ERR_CUDA;
@@ -118,6 +124,7 @@ void upload_batch(xpir_b200_server *srv, uint32_t lane, std::vector<xpir::Job *>
   if (e == cudaSuccess) e = cudaEventRecord(q0->uploaded, cs);
   if (e != cudaSuccess) {
     (void)cudaGetLastError();
+    report("upload", lane, e);
     for (auto *j : batch) {
       auto *q = (ServedQuery *)j->payload.get();
       q->upload_status = status_of_error(e);
@@ -166,12 +173,15 @@ void compute_batch(xpir_b200_server *srv, uint32_t lane, std::vector<xpir::Job *
     int s = run ? reqs[i].status : (upload != XPIR_B200_OK ? upload : status_of_error(e));
     if (!run && upload == XPIR_B200_OK) q->cuda_error = e;
     if (run && s == XPIR_B200_ERR_CUDA) q->cuda_error = ctx->last_error;
+    if (i == 0 && !run && upload == XPIR_B200_OK) report("wait for the upload", lane, e);
+    if (i == 0 && run && s == XPIR_B200_ERR_CUDA) report("batched reply", lane, ctx->last_error);
     if (s == XPIR_B200_OK) {
       q->nb_replies = reqs[i].nb_replies;
       const cudaError_t ce = cudaMemcpyAsync(q->host_replies, q->dr, q->reply_bytes, cudaMemcpyDeviceToHost, st);
       if (ce != cudaSuccess) {
         s = XPIR_B200_ERR_CUDA;
         q->cuda_error = ce;
+        report("reply copy to the host", lane, ce);
       }
     }
     batch[i]->status = s;
@@ -184,6 +194,7 @@ void compute_batch(xpir_b200_server *srv, uint32_t lane, std::vector<xpir::Job *
   }
   for (void *p : held) cudaFreeAsync(p, st);
   const cudaError_t se = cudaStreamSynchronize(st);
+  if (se != cudaSuccess) report("batch synchronisation", lane, se);
   if (se != cudaSuccess)
     for (auto *j : batch) {
       j->status = XPIR_B200_ERR_CUDA;
@@ -274,6 +285,7 @@ int xpir_b200_server_create(xpir_b200_server **out, xpir_b200_ctx *const *ctxs, 
       nctx, device_budget_bytes, max_batch,
       [srv](uint32_t lane, std::vector<xpir::Job *> &b) { upload_batch(srv, lane, b); },
       [srv](uint32_t lane, std::vector<xpir::Job *> &b) { compute_batch(srv, lane, b); }, 2));
+  for (xpir_b200_ctx *c : srv->ctxs) c->servers++;
   *out = srv;
   return XPIR_B200_OK;
 }
@@ -335,7 +347,8 @@ int xpir_b200_server_stats(xpir_b200_server *srv, uint64_t *completed, uint64_t 
 
 int xpir_b200_server_destroy(xpir_b200_server *srv) {
   if (!srv) return XPIR_B200_ERR_ARG;
-  srv->adm->stop();
+  srv->adm->stop(XPIR_B200_ERR_STATE);
+  for (xpir_b200_ctx *c : srv->ctxs) c->servers--;
   for (cudaStream_t cs : srv->copy_streams) cudaStreamDestroy(cs);
   for (cudaMemPool_t p : srv->pools) cudaMemPoolDestroy(p);
   delete srv;

@@ -73,4 +73,5 @@ __device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap *map) {
 bool encode_tensor_map_u64_4d(CUtensorMap *map, const void *base, const uint64_t dims[4], const uint64_t strides[3],
                               const uint32_t box[4]);
 
+
 }  // namespace xpir

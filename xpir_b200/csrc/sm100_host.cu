@@ -51,4 +51,12 @@ bool encode_tensor_map_u64_4d(CUtensorMap *map, const void *base, const uint64_t
   return r == CUDA_SUCCESS;
 }
 
+cudaError_t allow_max_dynamic_smem(const void *kernel) {
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  return e;
+}
+
 }  // namespace xpir
