@@ -65,6 +65,10 @@ WORKLOADS = {
     # ciphertexts, 6.55 GB) for element 54,321, PIRQueryGenerator with the reference's PRNG.
     "querygen": dict(N=2048, m=2, n=[100000], chosen=54321, sample=100000,
                      desc="query generation: LWE:80:2048:120, d=1, 100000 ciphertexts (6.55 GB) for element 54321"),
+    # Client-side extraction on the GPU: the replies to a d=1 query for one 50 MB element
+    # on the memory-bound parameter set (4,763 reply ciphertexts, 312 MB).
+    "extract": dict(N=2048, m=2, n=[100000], L=50_000_000,
+                    desc="extraction: LWE:80:2048:120, d=1, one 50 MB element (n0=100000)"),
     # Serving loop over three resident databases, one lane (context) each.  mix: (database,
     # d, alpha, weight) of the admitted shapes; grids from the client optimizer's rule.
     "serving": dict(dbs=[("DB1", 1024, 1, 200000, 2048), ("DB2", 2048, 2, 100000, 8192),
@@ -690,6 +694,110 @@ def querygen_arm(args, w: dict, world: int, rank: int, local: int) -> int:
     return 0
 
 
+def extract_replies(w: dict, moduli: list[int], seed: int):
+    """Synthetic replies of the extraction workload on the device: words in [0, 2p) per
+    modulus (the range of the reply chain's lazily reduced output)."""
+    import torch
+
+    from xpir_b200 import extract_count, bits_per_coeff
+
+    N, m = w["N"], w["m"]
+    b = bits_per_coeff(N, m, w["n"][0])
+    nct = extract_count(w["L"], len(w["n"]), b, N, m)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    r = torch.empty((nct, 2, m, N), dtype=torch.int64, device="cuda")
+    for c in range(m):
+        r[:, :, c, :].random_(0, 2 * moduli[c], generator=gen)
+    return r, b, nct
+
+
+def extract_arm(args, w: dict, world: int, rank: int, local: int) -> int:
+    """Client-side extraction (xpir_b200_extract) of one element's d=1 replies, device
+    resident (value) and from pinned host memory to host memory (e2e); ciphertexts/s."""
+    import torch
+
+    import xpir_b200
+    from oracle import pyoracle as po
+
+    dist = init_dist(world, local)
+    torch.cuda.set_device(local)
+    N, m, L = w["N"], w["m"], w["L"]
+    moduli = xpir_b200.moduli(m)
+    ctx = xpir_b200.Context(N, m, device=local)
+    sk = ctx.generate_secret_key(po.seeded_prng_key(11 + rank), 0)
+    dct, b, nct = extract_replies(w, moduli, 77 + rank)
+    dout = torch.empty(L, dtype=torch.uint8, device=f"cuda:{local}")
+    stream = torch.cuda.ExternalStream(ctx.stream, device=local)
+    for _ in range(args.warmup):
+        ctx.extract(sk, 1, b, L, dct, dout)
+    torch.cuda.synchronize()
+    launches0 = ctx.launch_count
+    if dist is not None:
+        dist.barrier()
+    with ClockSampler(local) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            ctx.extract(sk, 1, b, L, dct, dout)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = ctx.launch_count - launches0
+    # e2e: replies from pinned host memory, the element back to host memory
+    host_ct = torch.empty(dct.numel(), dtype=torch.int64, pin_memory=True)
+    host_ct.copy_(dct.view(-1))
+    host_out = torch.empty(L, dtype=torch.uint8, pin_memory=True)
+    hct, hout = host_ct.numpy().view(np.uint64), host_out.numpy()
+    ctx.extract(sk, 1, b, L, hct, hout)
+    torch.cuda.synchronize()
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        ctx.extract(sk, 1, b, L, hct, hout)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    ms, e2e_ms = max_over_ranks(dist, [ms, e2e_ms], f"cuda:{local}")
+    if rank == 0:
+        peaks = measured_peaks()
+        ct_bytes = 2 * m * N * 8
+        algo = nct * ct_bytes + L
+        achieved = algo / (ms / 1e3) / 1e9
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline and po.ref_available():
+            r = po.ref_extract_bench(N, m, w["n"], 1, L, 1000, host_ct.numpy().view(np.uint64),
+                                     threads=os.cpu_count() or 1)
+            cpu = {"value": round(nct / r["extract_s"], 2), "unit": "ciphertexts/s", "cores": r["omp_threads"],
+                   "kind": "reference", "cpu_model": po.host_cpu_model(),
+                   "sample": f"the same {nct} replies through the reference's PIRReplyExtraction::extractReply "
+                             f"(its own seeded key), {r['extract_s']:.3f} s"}
+        line = {
+            "metric": METRIC, "value": round(world * nct / (ms / 1e3), 1), "unit": "ciphertexts/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic: seeded reply words in [0, 2p); the secret key from the reference's Salsa20 stream",
+            "config": {"workload": w["desc"], "N": N, "moduli": m, "n": w["n"], "bits_per_coeff": b,
+                       "element_bytes": L, "reply_ciphertexts": nct,
+                       "l2": "inputs larger than L2 (no flush needed)",
+                       "parallelism": f"replicas{world}" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": None,
+                         "kernel": "decrypt_poly_kernel + lift_pack_kernel (replies read once, element written once)",
+                         "peak_source": peaks["source"], "algorithmic_bytes_per_launch": algo,
+                         "kernel_ms": round(ms, 4)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(world * nct / (e2e_ms / 1e3), 1), "unit": "ciphertexts/s",
+                    "h2d_bytes_per_step": nct * ct_bytes, "d2h_bytes_per_step": L, "ms_per_step": round(e2e_ms, 3)},
+            "gpu_launches": launches, "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
 def reference_batch_rate(w: dict, threads: int) -> dict:
     """The reference answering the batch's queries one at a time on the full database: one
     query of each class timed (xpir_ref bench, one repetition); the batch takes the sum of
@@ -1035,6 +1143,40 @@ def main() -> int:
         if args.impl == "reference":
             return reference_serving_arm(args, w, world, rank)
         return serving_arm(args, w, world, rank, local)
+    if args.workload == "extract":
+        if args.elements:
+            w.update(L=args.elements, desc=w["desc"].replace("one 50 MB element", f"one {args.elements}-byte element"))
+        if args.impl == "reference":
+            if rank != 0:
+                return 0
+            from oracle import pyoracle as po
+            import xpir_b200
+
+            if not po.ref_available():
+                print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/xpir_ref is not built "
+                                  "(extraction has no port timed in the oracle)"}))
+                return 0
+            b = xpir_b200.bits_per_coeff(w["N"], w["m"], w["n"][0])
+            nct = xpir_b200.extract_count(w["L"], 1, b, w["N"], w["m"])
+            rng = np.random.default_rng(77)
+            ct = np.empty((nct, 2, w["m"], w["N"]), dtype=np.uint64)
+            for c, p in enumerate(xpir_b200.moduli(w["m"])):
+                ct[:, :, c, :] = rng.integers(0, 2 * p, size=(nct, 2, w["N"]), dtype=np.uint64)
+            r = po.ref_extract_bench(w["N"], w["m"], w["n"], 1, w["L"], 1000, ct, threads=os.cpu_count() or 1)
+            v = round(nct / r["extract_s"], 2)
+            print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "ciphertexts/s",
+                              "n_gpus": args.gpus, "steps": 1, "warmup": 0,
+                              "ms_per_step": round(r["extract_s"] * 1e3, 3), "higher_is_better": True,
+                              "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+                              "data": "seeded reply words in [0, 2p); the reference's PIRReplyExtraction",
+                              "config": {"workload": w["desc"], "reply_ciphertexts": nct},
+                              "cpu_baseline": {"value": v, "unit": "ciphertexts/s", "cores": r["omp_threads"],
+                                               "kind": "reference", "cpu_model": po.host_cpu_model(),
+                                               "sample": "the whole reply set"},
+                              "e2e": {"value": v, "unit": "ciphertexts/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}))
+            return 0
+        return extract_arm(args, w, world, rank, local)
     if args.workload == "querygen":
         if args.elements:
             w.update(n=[args.elements], chosen=min(w["chosen"], args.elements - 1),

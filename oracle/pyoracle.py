@@ -376,6 +376,17 @@ def ref_extract(N: int, m: int, n: list[int], alpha: int, L: int, keyseed: int, 
         return np.fromfile(t / "p.bin", dtype=np.uint8)
 
 
+def ref_extract_bench(N: int, m: int, n: list[int], alpha: int, L: int, keyseed: int, reply: np.ndarray,
+                      threads: int | None = None) -> dict:
+    """The reference's PIRReplyExtraction::extractReply alone, timed with omp_get_wtime."""
+    with tempfile.TemporaryDirectory() as td:
+        t = Path(td)
+        np.ascontiguousarray(reply, dtype=np.uint64).tofile(t / "r.bin")
+        return _ref("extract", {"params": params_str(N, m), "alpha": alpha, "d": len(n), "n": ",".join(map(str, n)),
+                                "eltbytes": L, "keyseed": keyseed, "reply-in": t / "r.bin", "plain-out": t / "p.bin"},
+                    threads)
+
+
 def ref_key(N: int, m: int, keyseed: int) -> np.ndarray:
     """The reference's seeded secret key, [m][N] in the NTT domain."""
     with tempfile.TemporaryDirectory() as td:

@@ -366,7 +366,9 @@ int cmd_extract(const Args &a) {
     memcpy(x, r.data() + i * ct_bytes, ct_bytes);
     r_extractor->pushEncryptedReply(x);
   }
+  const double t0 = omp_get_wtime();
   r_extractor->extractReply(L);
+  const double t_extract = omp_get_wtime() - t0;
   uint64_t pb = r_extractor->getPlaintextReplyBytesize();
   uint64_t np = r_extractor->getnbPlaintextReplies(L);
   std::vector<char> plain(np * pb);
@@ -379,6 +381,8 @@ int cmd_extract(const Args &a) {
   write_file(a.str("plain-out"), plain.data(), L * params.alpha);
   delete r_extractor;
   delete crypto;
+  result("{\"replies\": %llu, \"extract_s\": %.6f, \"omp_threads\": %d}\n", (unsigned long long)nrep, t_extract,
+         omp_get_max_threads());
   return 0;
 }
 

@@ -42,20 +42,39 @@ struct LiftConsts {
   uint64_t P[kLimbs];              // product of the moduli
   uint64_t M[kMaxLiftModuli][kLimbs];
   uint64_t inv[kMaxLiftModuli];    // M_c^-1 mod p_c
+  uint64_t inv_shoup[kMaxLiftModuli];  // floor(inv * 2^64 / p_c)
 };
 
-__device__ __forceinline__ uint64_t limbs_mod(const uint64_t *x, uint64_t p) {
-  unsigned __int128 r = 0;
+// Exact reductions modulo one of XPIR's moduli (2^60 < p < 2^61 with D = 2^61 - p below
+// 2^23 for all 17 of them), which give the unique residue the reference's GMP lift
+// computes.  A 64-bit word w: q0 = w >> 61 <= 7 and w - q0*p = (w mod 2^61) + q0*D lies
+// in [0, 2p) whenever 9*D < 2^61.
+__device__ __forceinline__ uint64_t mod_word(uint64_t w, uint64_t p, uint64_t np) {
+  const uint64_t r = w + (w >> 61) * np;
+  return r >= p ? r - p : r;
+}
+
+// h*2^64 + l mod p for h < p: h*2^64 mod p = h*2^64 - f*p with f = floor(h*2^64/p) (the
+// Shoup factor of h), whose low word is f*(2^64 - p).
+__device__ __forceinline__ uint64_t mod_two_words(uint64_t h, uint64_t l, uint64_t p, uint64_t np, uint32_t delta) {
+  const uint64_t s = shoup_factor8_np(h, p, np, delta) * np + mod_word(l, p, np);  // < 2p
+  return s >= p ? s - p : s;
+}
+
+// x (its low nl of kLimbs little-endian limbs) mod p, from the top limb down; the loop is
+// unrolled over all limbs so that x stays in registers.
+__device__ __forceinline__ uint64_t limbs_mod_fast(const uint64_t (&x)[kLimbs], int nl, uint64_t p, uint64_t np,
+                                                   uint32_t delta) {
+  uint64_t r = 0;
 #pragma unroll
-  for (int i = kLimbs - 1; i >= 0; i--) r = ((r << 64) | x[i]) % p;
-  return (uint64_t)r;
+  for (int l = kLimbs - 1; l >= 0; l--) {
+    if (l == nl - 1) r = mod_word(x[l], p, np);
+    else if (l < nl - 1) r = mod_two_words(r, x[l], p, np, delta);
+  }
+  return r;
 }
 
-__device__ __forceinline__ uint64_t mulmod_u128(uint64_t a, uint64_t b, uint64_t p) {
-  return (uint64_t)(((unsigned __int128)a * b) % p);
-}
-
-__global__ void __launch_bounds__(256) decrypt_poly_kernel(const uint64_t *__restrict__ ct,
+__global__ void __launch_bounds__(256, 4) decrypt_poly_kernel(const uint64_t *__restrict__ ct,
                                                            const uint64_t *__restrict__ sk,
                                                            const uint64_t *__restrict__ sks,
                                                            const uint64_t *__restrict__ tables, uint32_t N,
@@ -68,7 +87,8 @@ __global__ void __launch_bounds__(256) decrypt_poly_kernel(const uint64_t *__res
   const uint64_t *a = ct + (j * 2 * m + c) * N, *b = ct + (j * 2 * m + m + c) * N;
   const uint64_t *s = sk + (uint64_t)c * N, *ss = sks + (uint64_t)c * N;
   const uint32_t shift = 32 - log_n;
-  for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {
+#pragma unroll 4
+  for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {  // unrolled: several rows of loads in flight
     const uint64_t temp = shoup_mac(0, a[i], s[i], ss[i], p);  // in [0, p)
     const uint64_t y = (temp < p) ? p - temp : p - temp % p;
     uint64_t z = b[i] + y;
@@ -81,10 +101,10 @@ __global__ void __launch_bounds__(256) decrypt_poly_kernel(const uint64_t *__res
                  [&](uint32_t k) { return poly[swz(k)]; });
   const uint64_t *iphi = tab + kInvPhi * N, *iphis = tab + kInvPhiShoup * N;
   uint64_t *o = res + (j * m + c) * N;
-  for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {
-    const uint32_t k = __brev(i) >> shift;
-    o[k] = shoup_mul(poly[swz(i)], iphi[k], iphis[k], p);
-  }
+  // In output order (coalesced global loads and stores); the bit reversal is its own
+  // inverse, so output k reads transform slot brev(k).
+  for (uint32_t k = threadIdx.x; k < N; k += blockDim.x)
+    o[k] = shoup_mul(poly[swz(__brev(k) >> shift)], iphi[k], iphis[k], p);
 }
 
 __global__ void __launch_bounds__(256) lift_pack_kernel(const uint64_t *__restrict__ res, uint64_t nct, uint32_t N,
@@ -94,11 +114,17 @@ __global__ void __launch_bounds__(256) lift_pack_kernel(const uint64_t *__restri
   if (t >= nct * N) return;
   const uint64_t j = t / N, i = t % N;
   uint64_t x[kLimbs] = {};
-  for (uint32_t c = 0; c < m; c++) {
-    const uint64_t p = dm.p[c];
-    const uint64_t r = res[(j * m + c) * N + i] % p;
-    const uint64_t have = c ? limbs_mod(x, p) : 0;
-    const uint64_t v = c ? mulmod_u128((r + p - have) % p, lc.inv[c], p) : r;
+#pragma unroll
+  for (uint32_t c = 0; c < kMaxLiftModuli; c++) {  // unrolled: static indexes into x and the constants
+    if (c >= m) break;
+    const uint64_t p = dm.p[c], np = 0 - p;
+    const uint32_t delta = (uint32_t)dm.shoup_delta[c];
+    const uint64_t r = mod_word(res[(j * m + c) * N + i], p, np);
+    // x < p_0*...*p_{c-1} < 2^(61c): ceil(61c/64) limbs
+    const uint64_t have = c ? limbs_mod_fast(x, (int)((61 * c + 63) / 64), p, np, delta) : 0;
+    uint64_t t = r + p - have;
+    t = t >= p ? t - p : t;
+    const uint64_t v = c ? shoup_mul(t, lc.inv[c], lc.inv_shoup[c], p) : r;
     unsigned __int128 carry = 0;  // x += M_c * v
 #pragma unroll
     for (int l = 0; l < kLimbs; l++) {
@@ -109,9 +135,10 @@ __global__ void __launch_bounds__(256) lift_pack_kernel(const uint64_t *__restri
   }
   // centred: x - P when 2x > P
   int cmp = 0;  // sign of 2x - P (x < P < 2^244: 2x fits the limbs)
-  for (int l = kLimbs - 1; l >= 0 && cmp == 0; l--) {
+#pragma unroll
+  for (int l = kLimbs - 1; l >= 0; l--) {  // unrolled (static limb indexes: registers)
     const uint64_t x2 = (x[l] << 1) | (l ? x[l - 1] >> 63 : 0);
-    if (x2 != lc.P[l]) cmp = x2 > lc.P[l] ? 1 : -1;
+    if (cmp == 0 && x2 != lc.P[l]) cmp = x2 > lc.P[l] ? 1 : -1;
   }
   unsigned __int128 v = ((unsigned __int128)x[1] << 64) | x[0];
   if (cmp > 0) v -= ((unsigned __int128)lc.P[1] << 64) | lc.P[0];
@@ -195,15 +222,16 @@ extern "C" int xpir_b200_extract(xpir_b200_ctx *ctx, const uint64_t *secret_key,
   if (m > kMaxLiftModuli || bits == 0 || bits >= 128 || bits >= 61 * m || (uint64_t)bits * N % 64 != 0)
     return XPIR_B200_ERR_ARG;
   if (capacity_bytes < aggregated_bytes) return XPIR_B200_ERR_ARG;
+  for (uint32_t c = 0; c < m; c++) {  // the lift's reductions (mod_word, mod_two_words) assume these
+    const uint64_t p = ps.mod[c].p;
+    if (p <= (1ull << 60) || p >= (1ull << 61) || (1ull << 61) - p >= (1ull << 57) || !shoup_factor_ok(p))
+      return XPIR_B200_ERR_ARG;
+  }
   const uint64_t top = extract_count(aggregated_bytes, d, bits, N, m);
   if (nb_replies < top) return XPIR_B200_ERR_ARG;
   const uint64_t mN = (uint64_t)m * N, ct_words = 2 * mN, abs_words = (uint64_t)bits * N / 64;
 
-  // Host constants: the key's Shoup factors and the mixed-radix lift.
-  std::vector<uint64_t> sks(mN);
-  for (uint32_t c = 0; c < m; c++)
-    for (uint32_t i = 0; i < N; i++)
-      sks[(uint64_t)c * N + i] = (uint64_t)(((unsigned __int128)secret_key[(uint64_t)c * N + i] << 64) / ps.mod[c].p);
+  // Host constants of the mixed-radix lift (the key's Shoup factors are computed on the device).
   LiftConsts lc;
   memset(&lc, 0, sizeof(lc));
   lc.P[0] = 1;
@@ -211,6 +239,7 @@ extern "C" int xpir_b200_extract(xpir_b200_ctx *ctx, const uint64_t *secret_key,
     const uint64_t p = ps.mod[c].p;
     memcpy(lc.M[c], lc.P, sizeof(lc.P));
     lc.inv[c] = c ? powmod_host(limbs_mod_host(lc.P, p), p - 2, p) : 1;
+    lc.inv_shoup[c] = (uint64_t)(((unsigned __int128)lc.inv[c] << 64) / p);
     limbs_mul_small(lc.P, p);
   }
   const DevModuli dm = make_dev_moduli(ps);
@@ -230,7 +259,10 @@ extern "C" int xpir_b200_extract(xpir_b200_ctx *ctx, const uint64_t *secret_key,
   e = cudaMallocFromPoolAsync((void **)&d_sk, mN * 8, ctx->pool, st);
   if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void **)&d_sks, mN * 8, ctx->pool, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_sk, secret_key, mN * 8, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(d_sks, sks.data(), mN * 8, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) {
+    e = launch_key_shoup(d_sk, d_sks, N, m, dm, st);
+    ctx->launches++;
+  }
   const uint64_t *level_in = (const uint64_t *)replies;
   if (e == cudaSuccess && !replies_on_device) {
     e = cudaMallocFromPoolAsync((void **)&d_in, top * ct_words * 8, ctx->pool, st);

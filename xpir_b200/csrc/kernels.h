@@ -51,6 +51,11 @@ struct ImportRows {
   uint64_t rows, per_row, active;
 };
 
+// The secret key's Shoup factors (sks = floor(sk * 2^64 / p), sk words below p) for
+// query generation and extraction, computed on the device on `stream`.
+cudaError_t launch_key_shoup(const uint64_t *sk, uint64_t *sks, uint32_t N, uint32_t m, const DevModuli &dm,
+                             cudaStream_t stream);
+
 // Lets `kernel` take up to the current device's opt-in maximum of dynamic shared memory.
 // For a kernel whose shared memory depends on the parameter set (import, extraction,
 // query generation), every caller sets this same value: contexts of different parameter

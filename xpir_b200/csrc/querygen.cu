@@ -151,6 +151,15 @@ __global__ void __launch_bounds__(256, 4) encrypt_kernel(const QueryGenArgs g, c
   }
 }
 
+// The secret key's Shoup factors floor(s*2^64/p) (s < p), on the device.
+__global__ void __launch_bounds__(256) key_shoup_kernel(const uint64_t *__restrict__ sk, uint64_t *__restrict__ sks,
+                                                        uint32_t N, const DevModuli dm) {
+  const uint32_t c = blockIdx.y;
+  const uint64_t p = dm.p[c];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+    sks[(uint64_t)c * N + i] = shoup_factor8_np(sk[(uint64_t)c * N + i], p, 0 - p, (uint32_t)dm.shoup_delta[c]);
+}
+
 // NFLLWE's secret key (crypto/NFLLWE.cpp:108-116): the uniform poly of one PRNG call.
 __global__ void __launch_bounds__(256) keygen_kernel(const QueryGenArgs g, uint64_t nonce, uint32_t N,
                                                      const DevModuli dm, uint64_t *__restrict__ sk) {
@@ -179,6 +188,13 @@ int status_of(cudaError_t e) {
 uint64_t bound_mask(uint64_t bound) { return (1ULL << (unsigned int)std::ceil(std::log2((double)bound))) - 1; }
 
 }  // namespace
+
+cudaError_t launch_key_shoup(const uint64_t *sk, uint64_t *sks, uint32_t N, uint32_t m, const DevModuli &dm,
+                             cudaStream_t stream) {
+  key_shoup_kernel<<<dim3((N + 255) / 256, m), 256, 0, stream>>>(sk, sks, N, dm);
+  return cudaGetLastError();
+}
+
 }  // namespace xpir
 
 using namespace xpir;
@@ -222,10 +238,6 @@ extern "C" int xpir_b200_generate_query(xpir_b200_ctx *ctx, const uint8_t *prng_
     g.amp_shoup[c] = (uint64_t)(((unsigned __int128)g.amp[c] << 64) / p);
     g.uniform_mask[c] = bound_mask(p);
   }
-  std::vector<uint64_t> sks(mN);
-  for (uint32_t c = 0; c < m; c++)
-    for (uint32_t i = 0; i < N; i++)
-      sks[(uint64_t)c * N + i] = (uint64_t)(((unsigned __int128)secret_key[(uint64_t)c * N + i] << 64) / ps.mod[c].p);
   const DevModuli dm = make_dev_moduli(ps);
 
   std::lock_guard<std::mutex> lock(ctx->mu);
@@ -236,7 +248,10 @@ extern "C" int xpir_b200_generate_query(xpir_b200_ctx *ctx, const uint8_t *prng_
   e = cudaMallocFromPoolAsync((void **)&d_sk, mN * 8, ctx->pool, st);
   if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void **)&d_sks, mN * 8, ctx->pool, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_sk, secret_key, mN * 8, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(d_sks, sks.data(), mN * 8, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) {
+    e = launch_key_shoup(d_sk, d_sks, N, m, dm, st);
+    ctx->launches++;
+  }
   uint64_t *target = (uint64_t *)query;
   if (e == cudaSuccess && !out_on_device) {
     e = cudaMallocFromPoolAsync((void **)&d_out, nq * ct_bytes, ctx->pool, st);
