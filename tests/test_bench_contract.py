@@ -44,3 +44,14 @@ def test_query_generation_reference_arm():
     assert d["impl"] == "reference" and d["unit"] == "ciphertexts/s" and d["value"] > 0
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["value"] == d["value"]
     assert "3000 ciphertexts" in d["config"]["workload"]
+
+
+def test_extraction_reference_arm():
+    from oracle import pyoracle as po
+
+    d = run_reference_arm("--workload", "extract", "--elements", "2000000")
+    if not po.ref_available():
+        assert "unavailable" in d
+        return
+    assert d["impl"] == "reference" and d["unit"] == "ciphertexts/s" and d["value"] > 0
+    assert d["cpu_baseline"]["kind"] == "reference" and d["config"]["reply_ciphertexts"] > 0
