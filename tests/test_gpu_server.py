@@ -120,6 +120,14 @@ def test_large_pinned_query_is_pulled_and_exact(engine):
         pinned = torch.from_numpy(q.view(np.int64)).pin_memory()
         small, _ = make_load(engine, [(ca, (1024, 1)), (cb, (2048, 2))])
         with engine.Server([ca, cb], device_budget_bytes=4 << 30, max_batch=16) as srv:
+            # alone, each: the pinned query costs one launch more (the pull kernel)
+            deltas = []
+            for buf in (pinned.numpy().view(np.uint64), q):
+                before = cb.launch_count
+                outs, _ = serve_all(engine, srv, [(db, n, buf, want)], clients=1)
+                assert np.array_equal(outs[0], want)
+                deltas.append(cb.launch_count - before)
+            assert deltas[0] == deltas[1] + 1, deltas
             big = [(db, n, pinned.numpy().view(np.uint64), want), (db, n, q, want)]
             outs, _ = serve_all(engine, srv, big + small, clients=3)
         for (_, _, _, w), got in zip(big + small, outs):

@@ -88,14 +88,15 @@ __global__ void __launch_bounds__(kPullThreads) pull_host_kernel(const uint4 *__
   for (; i < n16; i += stride) dst[i] = src[i];
 }
 
-// The device address of a host buffer that is mapped pinned memory, or null.
-const void *mapped_device_address(const void *host) {
+// The address, on `device`, of a host buffer that is pinned memory mapped for that
+// device, or null (pageable memory, or pinned on behalf of another device).
+const void *mapped_device_address(const void *host, int device) {
   cudaPointerAttributes at;
   if (cudaPointerGetAttributes(&at, host) != cudaSuccess) {
     (void)cudaGetLastError();
     return nullptr;
   }
-  return at.type == cudaMemoryTypeHost ? at.devicePointer : nullptr;
+  return at.type == cudaMemoryTypeHost && at.device == device ? at.devicePointer : nullptr;
 }
 
 // Stage 1, on the admitting thread: the batch's query and reply buffers and the queries'
@@ -109,7 +110,7 @@ void upload_batch(xpir_b200_server *srv, uint32_t lane, std::vector<xpir::Job *>
     if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&q->dq, q->query_bytes ? q->query_bytes : 256, srv->pools[lane], cs);
     if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&q->dr, q->reply_bytes ? q->reply_bytes : 256, srv->pools[lane], cs);
     if (e != cudaSuccess) continue;
-    const void *mapped = q->query_bytes >= kPullBytes ? mapped_device_address(q->host_query) : nullptr;
+    const void *mapped = q->query_bytes >= kPullBytes ? mapped_device_address(q->host_query, ctx->device) : nullptr;
     if (mapped && (((uintptr_t)mapped | (uintptr_t)q->dq | q->query_bytes) & 15) == 0) {
       pull_host_kernel<<<kPullBlocks, kPullThreads, 0, cs>>>((const uint4 *)mapped, (uint4 *)q->dq,
                                                             q->query_bytes / 16);
