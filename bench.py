@@ -406,6 +406,7 @@ def measure_single(args, w: dict, world: int, rank: int, local: int, dist) -> di
 
     line = None
     if rank == 0:
+        pcie = h2d_gbs(device)
         peaks = measured_peaks()
         query_bytes = nq * ct_words * 8
         reply_bytes = Pl * ct_words * 8
@@ -457,7 +458,9 @@ def measure_single(args, w: dict, world: int, rank: int, local: int, dist) -> di
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 3), "unit": "GB/s", "h2d_bytes_per_step": query_bytes,
-                    "d2h_bytes_per_step": reply_bytes, "ms_per_step": round(e2e_ms, 3)},
+                    "d2h_bytes_per_step": reply_bytes, "ms_per_step": round(e2e_ms, 3),
+                    "pcie_h2d_gbs_measured": round(pcie, 2),
+                    "frac_of_pcie": round((query_bytes + reply_bytes) / (e2e_ms / 1e3) / 1e9 / pcie, 4)},
             "gpu_launches": launches,
             "clocks": clocks,
             "import": {"seconds_wall": round(import_s, 4), "input_bytes": F * L, "imported_bytes": db_bytes},
@@ -467,6 +470,25 @@ def measure_single(args, w: dict, world: int, rank: int, local: int, dist) -> di
     ctx.close()
     del q_dev, q_host, out_dev, out_host, flush_buf
     return line
+
+
+def h2d_gbs(device: int, nbytes: int = 1 << 30, reps: int = 3) -> float:
+    """Pinned host-to-device copy rate of this GPU's PCIe link (best of `reps` copies of
+    `nbytes`, CUDA events): the bound of the end-to-end steps, which move each step's query
+    across it."""
+    import torch
+
+    src = torch.empty(nbytes // 8, dtype=torch.int64, pin_memory=True)
+    dst = torch.empty(nbytes // 8, dtype=torch.int64, device=f"cuda:{device}")
+    best = float("inf")
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dst.copy_(src, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    return nbytes / (best / 1e3) / 1e9
 
 
 def sub_object(line: dict) -> dict:
