@@ -141,6 +141,8 @@ int xpir_b200_ctx_create(xpir_b200_ctx **out, int device, uint32_t N, uint32_t m
   if (rc == XPIR_B200_OK) rc = cuda_status(preload_reply_kernels());
   if (rc == XPIR_B200_OK) rc = cuda_status(prepare_noalloc_scratch(device));
   if (rc == XPIR_B200_OK) rc = cuda_status(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  if (rc == XPIR_B200_OK) rc = cuda_status(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+  if (rc == XPIR_B200_OK) rc = cuda_status(cudaEventCreateWithFlags(&ctx->query_copied, cudaEventDisableTiming));
   if (rc == XPIR_B200_OK) {
     cudaMemPoolProps props = {};
     props.allocType = cudaMemAllocationTypePinned;
@@ -190,6 +192,9 @@ int xpir_b200_ctx_destroy(xpir_b200_ctx *ctx) {
   for (auto &pair : ctx->timing_ev)
     for (cudaEvent_t ev : pair)
       if (ev) cudaEventDestroy(ev);
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+  if (ctx->query_copied) cudaEventDestroy(ctx->query_copied);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
   delete ctx;
@@ -390,9 +395,28 @@ int xpir_b200_reply(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, cons
   if ((rc = grow(&ctx->ws_b, &ctx->ws_b_bytes, need_b)) != XPIR_B200_OK) return rc;
 
   const uint64_t *dq = (const uint64_t *)query;
+  const bool split_copy = !query_on_device && d > 1;
+  // Every return waits for the copy stream, so that no copy from the caller's query is
+  // left in flight (on success it has long finished: level 2 waited for it).
+  struct CopyGuard {
+    cudaStream_t s;
+    bool on;
+    ~CopyGuard() {
+      if (on) cudaStreamSynchronize(s);
+    }
+  } copy_guard{ctx->copy_stream, split_copy};
   if (!query_on_device) {
     if ((rc = grow(&ctx->ws_query, &ctx->ws_query_bytes, total_ct * ct_bytes)) != XPIR_B200_OK) return rc;
-    XPIR_TRY(cudaMemcpyAsync(ctx->ws_query, query, total_ct * ct_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    // The first level's ciphertexts on the context's stream; the other levels' on the copy
+    // stream, so that the first level's reply runs while they cross PCIe (the level loop
+    // waits for them before level 2).
+    const uint64_t first = (uint64_t)n[0] * ct_bytes;
+    XPIR_TRY(cudaMemcpyAsync(ctx->ws_query, query, first, cudaMemcpyHostToDevice, ctx->stream));
+    if (split_copy) {
+      XPIR_TRY(cudaMemcpyAsync((char *)ctx->ws_query + first, (const char *)query + first,
+                               (total_ct - n[0]) * ct_bytes, cudaMemcpyHostToDevice, ctx->copy_stream));
+      XPIR_TRY(cudaEventRecord(ctx->query_copied, ctx->copy_stream));
+    }
     dq = (const uint64_t *)ctx->ws_query;
   }
 
@@ -414,6 +438,7 @@ int xpir_b200_reply(xpir_b200_ctx *ctx, const xpir_b200_db *db, uint32_t d, cons
     const bool last = lvl + 1 == d;
     uint64_t *rep = (last && out_on_device) ? (uint64_t *)replies : (uint64_t *)ctx->ws_a;
     uint32_t launched = 0;
+    if (lvl == 1 && split_copy) XPIR_TRY(cudaStreamWaitEvent(ctx->stream, ctx->query_copied, 0));
     ReplyLevelArgs a{in, in_real, Ps[lvl], groups[lvl], n[lvl], dq, rep};
     a.write_idle = last;
     a.wait_test = ctx->wait_test;

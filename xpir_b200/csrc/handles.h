@@ -26,6 +26,10 @@ typedef std::map<std::tuple<uint64_t, uint64_t, uint64_t>, int> TuneTable;
 struct xpir_b200_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // Host queries of recursive replies: the later levels' ciphertexts are copied on this
+  // stream while the first level replies; the event marks the end of that copy.
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t query_copied = nullptr;
   xpir::ParamSet ps;           // b is set per database
   uint64_t *d_tables = nullptr;
   std::mutex mu;
