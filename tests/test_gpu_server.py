@@ -144,3 +144,36 @@ def test_context_outlives_its_server(engine):
     assert ctx.launch_count >= 0  # still alive
     ctx.close()
     assert srv.handle is None and ctx.handle is None
+
+
+def test_parameter_sets_launch_concurrently(engine):
+    """Contexts of different parameter sets running recursive replies (import and re-import
+    kernels whose shared memory depends on N) from several threads at once: every call
+    succeeds and equals its single-threaded result (a per-launch shared-memory attribute
+    set by one thread between another's setting and launch once made such launches fail)."""
+    specs = [(1024, 1, [12, 8], 900), (4096, 3, [10, 6], 700), (2048, 2, [14, 5], 800)]
+    work = []
+    for k, (N, m, n, L) in enumerate(specs):
+        ctx = engine.Context(N, m)
+        F = n[0] * n[1]
+        b = engine.bits_per_coeff(N, m, n[0])
+        db = ctx.import_db(random_db(500 + k, F, L), F, L, 1, b)
+        q = random_query(600 + k, n, N, m, engine.moduli(m))
+        work.append((ctx, db, n, q, ctx.reply(db, n, q)))
+    errors = []
+
+    def run(ctx, db, n, q, want):
+        try:
+            for _ in range(25):
+                assert np.array_equal(ctx.reply(db, n, q), want)
+        except Exception as e:  # reported in the test's thread
+            errors.append(e)
+
+    threads = [threading.Thread(target=run, args=w) for w in work for _ in range(2)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for ctx, *_ in work:
+        ctx.close()
+    assert not errors, errors[:3]
